@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Benchmark: OpenVort's velocity + RK4 path on the large periodic tangle.
+
+Workload (one "step" = one RK4 step = 4 velocity evaluations: k1 by
+update_tangle, then three stages, each with its own octree build):
+  ~1M points: rings with centres uniform in a periodic cube D = 0.4 cm,
+  orientations uniform on the sphere, radii uniform in [0.02, 0.05] D,
+  spacing dl = D/800; 26 nearest periodic images; Barnes-Hut theta = 0.5;
+  counterflow v_n = 0.5 cm/s along x, alpha = 0.098, alpha' = 0.016;
+  dt = 1e-6 s; mixed precision (FP32 far field, FP64 positions / local term /
+  near segments).  Seeded synthetic data.
+
+Printed JSON line (rank 0): value = point-velocity evaluations per second
+over all GPUs (N points x 4 evaluations per step / device time), plus RK4
+steps/s, the plain FP64 form's rate, the mixed-vs-FP64 error, the error
+against an FP64 direct sum on 4096 sample nodes, the roofline of the
+Barnes-Hut walk kernel, the reference's CPU baseline, the end-to-end rate
+through the reference-named C ABI with pinned host buffers, launches and
+clocks.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "point-velocity evals/s & RK4 steps/s at 1M pts: mixed vs FP64, ≤1e-5 rel err"
+UNIT = "point-velocity evals/s"
+D = 0.4
+DL = D / 800
+FLOPS_P2P = 43.0   # per segment-point interaction (direct sum / tree leaves)
+FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--points", type=int, default=1_000_000)
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--dt", type=float, default=1e-6)
+    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def params(theta):
+    from openvort_b200.tangle import Flow, Params
+    return Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=2 * DL, hyperfriction=1,
+                  max_curv_scale=0.2, hyperalpha=0.5, use_bh=1, bh_theta=theta, bh_grain=1e-8,
+                  vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}), vs=Flow("no flow"))
+
+
+def make_tangle(points, seed, alloc=np.empty):
+    from openvort_b200 import geometry as G
+    n_rings = G.rings_for_points(points, D, dl=DL)
+    return G.random_ring_tangle(seed, n_rings, D, dl=DL, boundary="periodic-26", alloc=alloc), n_rings
+
+
+def pinned_alloc():
+    import torch
+
+    keep = []
+
+    def alloc(shape, dtype):
+        tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.int32): torch.int32}[np.dtype(dtype)]
+        t = torch.empty(shape, dtype=tdt, pin_memory=True)
+        keep.append(t)
+        return t.numpy()
+
+    return alloc, keep
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (every 200 ms)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local)
+        dist_mod.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                    timeout=__import__("datetime").timedelta(seconds=600))
+        dist = dist_mod
+    return world, rank, local, dist
+
+
+def max_over_ranks(dist, x: float) -> float:
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    import torch
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_reference_sample(tangle, p, target_s=10.0, time0=0.0):
+    """The reference's own per-evaluation work (update_tangents_normals,
+    octree_build, update_velocity on a seeded sample of nodes, OpenMP over all
+    host cores) from oracle/_ref; returns point-evals/s extrapolated to the
+    whole tangle and a description."""
+    from oracle.oracle import Ref, have_ref
+    if not have_ref():
+        return None
+    threads = os.cpu_count() or 1
+    ref = Ref(threads=threads)
+    ref.configure(p)
+    t = tangle.copy()
+    t.set_images_from_library(ref.lib)
+    f = ref.lib.refh_sample_eval
+    f.restype = None
+    f.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                  C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    rng = np.random.default_rng(7)
+    act = np.nonzero(t.active)[0]
+    tg, tb, tn = C.c_double(), C.c_double(), C.c_double()
+    # probe with a few nodes, then size the sample for ~target_s of node work
+    m = 64
+    idx = np.ascontiguousarray(rng.choice(act, size=m, replace=False).astype(np.int32))
+    f(C.cast(t.ptr(), C.c_void_p), time0, idx.ctypes.data, m, C.byref(tg), C.byref(tb), C.byref(tn))
+    per = max(tn.value / m, 1e-7)
+    m = int(min(len(act), max(64, target_s / per)))
+    idx = np.ascontiguousarray(rng.choice(act, size=m, replace=False).astype(np.int32))
+    f(C.cast(t.ptr(), C.c_void_p), time0, idx.ctypes.data, m, C.byref(tg), C.byref(tb), C.byref(tn))
+    n = len(act)
+    t_eval = tg.value + tb.value + tn.value * n / m
+    return {"value": n / t_eval, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": (f"reference update_tangents_normals + octree_build on all {n} nodes "
+                       f"({tg.value:.2f} s + {tb.value:.2f} s) and update_velocity on {m} seeded nodes "
+                       f"({tn.value:.2f} s, OpenMP {threads} threads), extrapolated to one evaluation "
+                       f"of all nodes: {t_eval:.1f} s")}
+
+
+def run_reference_arm(args, world, rank):
+    p = params(args.theta)
+    tangle, n_rings = make_tangle(args.points, args.seed)
+    vals = []
+    # warm-up samples are small; each timed step is one sampled evaluation
+    for _ in range(args.warmup):
+        cpu_reference_sample(tangle, p, target_s=0.5)
+    for _ in range(args.steps):
+        r = cpu_reference_sample(tangle, p, target_s=8.0)
+        if r is None:
+            print(json.dumps({"impl": "reference",
+                              "unavailable": "oracle/_ref/libov_ref.so (reference compiled from its sources) is not built"}))
+            return
+        vals.append(r)
+    v = statistics.median([r["value"] for r in vals])
+    n = int(tangle.active.sum())
+    ms_step = 4 * n / v * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"large periodic tangle, {n} points ({n_rings} rings, D=0.4 cm, dl=D/800), "
+                                   f"26 images, Barnes-Hut theta={args.theta}", "points": n,
+                       "theta": args.theta},
+            "rk4_steps_per_s": 1e3 / ms_step,
+            "cpu_baseline": {**vals[-1], "value": v},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    world, rank, local, dist = dist_setup(args)
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference_arm(args, world, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    import torch
+    import openvort_b200 as ov
+    from openvort_b200 import _lib
+
+    lib = ov.load()
+    if lib.ov_init(local) != 0:
+        raise SystemExit(f"libov_gpu: {lib.ov_last_error_message().decode()}")
+    torch.cuda.set_device(local)
+    p = params(args.theta)
+    tangle, n_rings = make_tangle(args.points, args.seed + 1000 * rank)
+    n = int(tangle.active.sum())
+
+    # ---------------- device-resident timing, mixed precision
+    ov.configure(p, ov.OV_PREC_MIXED)
+    st = ov.DeviceState(tangle.copy())
+    st.run(0.0, args.dt, args.warmup)
+    barrier(dist)
+    st.reset_stats()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(dist)
+    st.run(args.warmup * args.dt, args.dt, args.steps)
+    barrier(dist)
+    clk = clocks.stop()
+    rs = st.stats()
+    ms_run = max_over_ranks(dist, rs.last_run_ms)
+    ms_step = ms_run / args.steps
+    value = world * n * 4 * args.steps / (ms_run / 1e3)
+    # roofline of the Barnes-Hut walk: algorithmic flops per launch / device
+    # time per launch (CUDA events around each walk launch on its stream)
+    flops = rs.interactions * FLOPS_P2P + rs.cell_interactions * FLOPS_CELL
+    walk_ms = rs.bs_kernel_ms / max(1.0, rs.bs_launches)
+    achieved = flops / max(1.0, rs.bs_launches) / (walk_ms / 1e3) / 1e12
+    peak32 = C.c_double(0)
+    lib.ov_measure_fma_peak(0, C.byref(peak32))
+    launches = int(rs.launches)
+    walk_share = rs.bs_kernel_ms / ms_run if ms_run > 0 else None
+    build_share = rs.build_ms / ms_run if ms_run > 0 else None
+    st.close()
+
+    # ---------------- plain FP64 form, same workload
+    ov.configure(p, ov.OV_PREC_FP64)
+    st64 = ov.DeviceState(tangle.copy())
+    st64.run(0.0, args.dt, 1)
+    barrier(dist)
+    st64.reset_stats()
+    barrier(dist)
+    st64.run(args.dt, args.dt, args.fp64_steps)
+    barrier(dist)
+    rs64 = st64.stats()
+    ms64 = max_over_ranks(dist, rs64.last_run_ms) / args.fp64_steps
+    value64 = world * n * 4 / (ms64 / 1e3)
+    peak64 = C.c_double(0)
+    lib.ov_measure_fma_peak(1, C.byref(peak64))
+    flops64 = rs64.interactions * FLOPS_P2P + rs64.cell_interactions * FLOPS_CELL
+    ach64 = flops64 / max(1.0, rs64.bs_launches) / (rs64.bs_kernel_ms / max(1.0, rs64.bs_launches) / 1e3) / 1e12
+    st64.close()
+
+    # ---------------- accuracy: mixed vs FP64 (all nodes), and both vs an
+    # FP64 direct sum (no tree) on 4096 seeded sample nodes
+    err = {}
+    if rank == 0:
+        def vel(prec):
+            ov.configure(p, prec)
+            s = ov.DeviceState(tangle.copy())
+            s.update_tangle(0.0)
+            s.download()
+            v = s.t.vels.copy()
+            s.close()
+            return v
+        v64, vmx = vel(ov.OV_PREC_FP64), vel(ov.OV_PREC_MIXED)
+        act = tangle.active
+        num = np.linalg.norm(vmx[act] - v64[act], axis=1)
+        den = np.linalg.norm(v64[act], axis=1)
+        err["max_rel_err_mixed_vs_fp64"] = float(np.max(num / den))
+        rng = np.random.default_rng(4096)
+        idx = rng.choice(np.nonzero(act)[0], size=min(4096, int(act.sum())), replace=False).astype(np.int32)
+        pts = tangle.pos[idx]
+        ov.configure(p, ov.OV_PREC_FP64)
+        s = ov.DeviceState(tangle.copy())
+        direct = s.eval_points(pts, idx, method=0)
+        bh64 = s.eval_points(pts, idx, method=1)
+        ov.configure(p, ov.OV_PREC_MIXED)
+        s2 = ov.DeviceState(tangle.copy())
+        bhmx = s2.eval_points(pts, idx, method=1)
+        s.close()
+        s2.close()
+
+        def rel(a, b):
+            return float(np.max(np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)))
+        err["bs_rel_err_bh_fp64_vs_direct_4096"] = rel(bh64, direct)
+        err["bs_rel_err_bh_mixed_vs_direct_4096"] = rel(bhmx, direct)
+        err["bs_rel_err_bh_mixed_vs_bh_fp64_4096"] = rel(bhmx, bh64)
+
+    # ---------------- end to end through the reference-named C ABI, pinned
+    # host buffers: update_tangle + rk4_step copy in and out every call
+    e2e = None
+    if not args.no_e2e:
+        alloc, keep = pinned_alloc()
+        ht = tangle.copy(alloc=alloc)
+        ov.configure(p, ov.OV_PREC_MIXED)
+        ov.update_tangle(ht, 0.0)
+        ov.rk4_step(ht, 0.0, args.dt)
+        barrier(dist)
+        t0 = time.perf_counter()
+        tt = args.dt
+        for _ in range(args.steps):
+            ov.update_tangle(ht, tt)
+            ov.rk4_step(ht, tt, args.dt)
+            tt += args.dt
+        barrier(dist)
+        sec = max_over_ranks(dist, time.perf_counter() - t0)
+        N = ht.n
+        h2d = N * (40 + 88 + 64)      # geometry, velocities, rk4 inputs
+        d2h = N * (56 + 48 + 24)      # dxi+tangents+normals, vels+vs, positions
+        e2e = {"value": world * n * 4 * args.steps / sec, "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": sec / args.steps * 1e3,
+               "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
+                       "in pinned host memory"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_sample(tangle, p, target_s=10.0)
+
+    traffic = None
+    tfile = ROOT / "profiles" / "bh_walk_traffic.json"
+    if tfile.exists():
+        try:
+            tr = json.loads(tfile.read_text())
+            traffic = tr["dram_bytes_per_launch_per_point"] * n
+        except Exception:
+            traffic = None
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"large periodic tangle: {n} points per GPU ({n_rings} rings, D=0.4 cm, "
+                                   f"dl=D/800, radii U[0.02,0.05]D), 26 periodic images, Barnes-Hut "
+                                   f"theta={args.theta}, mixed FP32/FP64, RK4 dt={args.dt}",
+                       "points": n, "theta": args.theta, "images": 26, "dt": args.dt,
+                       "parallelism": f"{world} independent tangles (one per GPU)" if world > 1 else "1 GPU",
+                       "l2": "working set (octree cells + node table) larger than the 126 MB L2"},
+            "rk4_steps_per_s": world * 1e3 / ms_step,
+            "fp64": {"value": value64, "ms_per_step": ms64, "rk4_steps_per_s": world * 1e3 / ms64,
+                     "roofline_frac_of_fp64_peak": ach64 / peak64.value if peak64.value else None,
+                     "fp64_fma_peak_tflops": peak64.value},
+            "mixed_over_fp64_speedup": ms64 / ms_step,
+            **err,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak32.value if peak32.value else None, "traffic": traffic,
+                         "kernel": "k_walk_nodes<mixed> (Barnes-Hut walk, 27 walks per point)",
+                         "peak_source": "ov_measure_fma_peak: FP32 FMA burst on this GPU, this run",
+                         "flops_per_launch": flops / max(1.0, rs.bs_launches),
+                         "launch_ms": walk_ms, "share_of_step": walk_share,
+                         "tree_build_share_of_step": build_share},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

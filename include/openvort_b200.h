@@ -1,0 +1,296 @@
+/*
+ * openvort_b200.h - C ABI of libov_gpu.so, the B200 (sm_100a) implementation
+ * of OpenVort's Schwarz vortex-filament velocity and RK4 path.
+ *
+ * Part 1 keeps the reference's own data layouts and prototypes so the library
+ * is a drop-in for the reference's hot path: a program built from the
+ * reference's remaining C files (main.c, reconnection, remeshing, I/O) links
+ * against libov_gpu.so instead of tangle.c's velocity functions, octree.c and
+ * vortex_dynamics.c's stepping.  Every declaration cites the reference
+ * interface it replaces (paths relative to the OpenVort checkout).
+ *
+ * Part 2 adds entry points the reference has no counterpart for: device
+ * selection and error reporting, precision control, a device-resident state
+ * for multi-step runs, batched independent systems, point queries, and the
+ * adjoint.
+ *
+ * Error convention: the reference's functions return void and abort through
+ * error() (src/util.c:29-34).  Here every failure (no GPU, CUDA error, bad
+ * input, non-finite result, tree too deep, spin-wait limit) is recorded in a
+ * per-thread status read by ov_last_error(), printed to stderr, and, when the
+ * environment variable OV_ABORT_ON_ERROR=1, aborts like the reference.
+ * Outputs of a failed call are not written.  There is no CPU fallback.
+ */
+#ifndef OPENVORT_B200_H
+#define OPENVORT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ===================================================================== */
+/* Part 1: reference-compatible layouts and prototypes                    */
+/* ===================================================================== */
+
+/* The include guards below are the reference headers' own, so this header
+ * and the reference's headers can be included in either order. */
+#ifndef VEC3_MATHS_H
+#define VEC3_MATHS_H
+/* include/vec3_maths.h:23-68 */
+struct vec3d { double p[3]; };
+struct mat3d { double m[3][3]; };
+struct segment { struct vec3d r1, r2; };
+typedef enum _wt { WALL_OPEN, WALL_PERIODIC, WALL_MIRROR } wall_type;
+typedef enum _fc { NOT_A_FACE = -1, X_L, X_H, Y_L, Y_H, Z_L, Z_H } boundary_faces;
+struct domain_box {
+  struct vec3d bottom_left_back;
+  struct vec3d top_right_front;
+  wall_type wall[6];
+};
+#endif
+
+#ifndef TANGLE_H
+#define TANGLE_H
+/* include/tangle.h:28-106 */
+typedef enum _ns_e { EMPTY = -1, FREE, PINNED, PINNED_SLIP } node_status_t;
+typedef struct _ns { node_status_t status; boundary_faces pin_wall; } node_status;
+struct neighbour_t { int forward; int reverse; };
+struct image_tangle { int shift[3]; int reflect; };
+struct boundary_images { const struct image_tangle *images; int n; };
+struct tangle_state {
+  struct vec3d *vnodes;
+  struct vec3d *vnodes_new;
+  struct vec3d *vels;
+  struct vec3d *vs;
+  struct vec3d *tangents;
+  struct vec3d *normals;
+  double *dxi;
+  int *recalculate;
+  struct neighbour_t *connections;
+  node_status *status;
+  struct domain_box box;
+  struct boundary_images bimg;
+  int N;
+  int next_free;
+  int total_free;
+};
+
+/* boundary image tables (include/tangle.h:62-77, src/boundary_images.c).
+ * Same images, order and counts as the reference, except wall_1_6: the
+ * reference declares n=6 over a 5-entry array (reads past its end); here
+ * n=5. */
+extern const struct boundary_images open_boundaries;
+extern const struct boundary_images periodic_6;
+extern const struct boundary_images periodic_18;
+extern const struct boundary_images periodic_26;
+extern const struct boundary_images periodic_z_open_xy;
+extern const struct boundary_images wall_1_open;
+extern const struct boundary_images wall_1_6;
+extern const struct boundary_images wall_1_18;
+extern const struct boundary_images wall_1_26;
+extern const struct boundary_images wall_2_4;
+extern const struct boundary_images wall_2_2;
+extern const struct boundary_images wall_2_26;
+extern const struct boundary_images channel_z;
+
+struct octree;
+
+/* image point of r (include/tangle.h:116-117, src/tangle.c:39-79) */
+struct vec3d shifted(const struct image_tangle *shift,
+                     const struct tangle_state *tangle, const struct vec3d *r);
+/* include/tangle.h:119-120, src/tangle.c:245-480,704-727.
+ * update_tangents_normals computes dxi, tangents and normals of every node on
+ * the GPU.  update_tangent_normal(k) computes the same for the whole tangle
+ * from the current positions and writes back node k's tangent and normal. */
+void update_tangent_normal(struct tangle_state *tangle, size_t k);
+void update_tangents_normals(struct tangle_state *tangle);
+/* include/tangle.h:128, src/tangle.c:686-702: velocities of all nodes
+ * (LIA + external + direct or Barnes-Hut Biot-Savart + boundary images +
+ * hyperfriction + mutual friction).  tree: NULL builds a tree internally when
+ * global_use_BH; otherwise a tree from octree_build. */
+void update_velocities(struct tangle_state *tangle, double t, struct octree *tree);
+/* include/tangle.h:136, src/tangle.c:583-684: one node (used by the
+ * reference's reconnection).  One GPU launch per call. */
+void update_velocity(struct tangle_state *tangle, int k, double t, struct octree *tree);
+/* include/tangle.h:142,152-153, src/tangle.c:553-581 */
+struct vec3d calculate_vs(struct tangle_state *tangle, struct vec3d r, int skip);
+struct vec3d calculate_vs_shift(const struct tangle_state *tangle, struct vec3d r,
+                                int skip, const struct vec3d *shift,
+                                const int *use_only_points, const int Npoints);
+#endif /* TANGLE_H */
+
+#ifndef INCLUDE_OCTREE_H_
+#define INCLUDE_OCTREE_H_
+/* include/octree.h:36-48.  struct octree is opaque here: the tree lives in
+ * device memory.  Only the reference's octree.c reads its fields, and this
+ * library replaces octree.c.  The tree keeps a snapshot of the node
+ * positions taken by octree_build. */
+struct octree *octree_build(const struct tangle_state *tangle, int quadtree);
+void octree_destroy(struct octree *tree);
+void octree_get_vs(const struct octree *tree, const struct vec3d *r,
+                   double resolution, struct vec3d *res, int skip);
+#endif
+
+#ifndef VORTEX_DYNAMICS
+#define VORTEX_DYNAMICS
+/* include/vortex_dynamics.h:47-49, src/vortex_dynamics.c:36-121.
+ * rk4_step needs tangle->vels to hold the velocities at the current
+ * positions (as the reference does) and updates tangle->vnodes only. */
+void euler_step(struct tangle_state *tangle, double dt);
+void rk4_step(struct tangle_state *tangle, double t, double dt);
+#endif
+
+#ifndef EXTERNAL_VELOCITY_H
+#define EXTERNAL_VELOCITY_H
+/* include/external_velocity.h:54-90.  The library reads vn_conf / vs_conf /
+ * vb_conf by their name and parameters (the host function pointer cannot run
+ * on the GPU) and evaluates the same 16 flows on the device. */
+#define scalar_param 1
+#define vector_param 2
+struct v_param_t {
+  char *name;
+  int type;
+  union param_value_t {
+    struct vec3d vector;
+    double scalar;
+  } value;
+};
+struct v_conf_t;
+typedef int (*get_v_t)(const struct vec3d *, double, struct vec3d *, struct v_conf_t *vconf);
+struct v_conf_t {
+  char *name;
+  get_v_t fun;
+  int n_params;
+  struct v_param_t v_params[32];
+};
+extern struct v_conf_t vn_conf;
+extern struct v_conf_t vs_conf;
+extern struct v_conf_t vb_conf;
+#endif
+
+/* Run-time globals the hot path reads (include/vortex_constants.h:25-78,
+ * defaults of src/vortex_constants.c:24-95).  Defined in libov_gpu.so with
+ * the reference's defaults; an executable that also links the reference's
+ * vortex_constants.o interposes its own definitions, which the library then
+ * reads. */
+extern double VORTEX_WIDTH;
+extern double KAPPA;
+extern int global_LIA_only;
+extern double global_alpha;
+extern double global_alpha_p;
+extern double global_dl_max;
+extern int global_num_threads;
+extern int global_use_mutual_friction;
+extern int global_use_BH;
+extern double global_BH_resolution;
+extern int global_BH_quadtree;
+extern double global_BH_grain;
+extern int global_hyperfriction;
+extern double global_max_curvature_scale;
+extern double global_hyperalpha;
+
+/* ===================================================================== */
+/* Part 2: extensions (no reference counterpart)                          */
+/* ===================================================================== */
+
+/* status codes */
+enum {
+  OV_OK = 0,
+  OV_ERR_NO_DEVICE = 1,   /* no CUDA device / library built without sm_100a */
+  OV_ERR_CUDA = 2,        /* CUDA runtime error */
+  OV_ERR_INVALID = 3,     /* bad argument or tangle (broken links, bad sizes) */
+  OV_ERR_NONFINITE = 4,   /* NaN/Inf in inputs or results */
+  OV_ERR_FLOW = 5,        /* unknown external flow name / missing parameter */
+  OV_ERR_TREE_DEPTH = 6,  /* box/BH_grain ratio needs more than 32 tree levels */
+  OV_ERR_TIMEOUT = 7,     /* a bounded device wait ran out */
+  OV_ERR_NOMEM = 8        /* device allocation failed */
+};
+
+/* precision modes */
+enum {
+  OV_PREC_FP64 = 0,  /* everything in FP64: the reference's arithmetic */
+  OV_PREC_MIXED = 1  /* FP32 far field, FP64 positions/local term/near field */
+};
+
+/* Select the CUDA device (default 0).  Called implicitly by the first call. */
+int ov_init(int device);
+int ov_last_error(void);
+const char *ov_last_error_message(void);
+const char *ov_error_string(int code);
+void ov_clear_error(void);
+
+/* precision of subsequent calls (process-wide); default OV_PREC_FP64 */
+void ov_set_precision(int mode);
+int ov_get_precision(void);
+/* 0 (default): the reference's RK4, whose fourth stage advances dt/2
+ * (src/vortex_dynamics.c:89); 1: classic RK4 (fourth stage advances dt) */
+void ov_set_rk4_classic(int classic);
+int ov_get_rk4_classic(void);
+
+/* Per-call counters of the last velocity evaluation on this thread. */
+typedef struct {
+  double interactions;      /* segment-point interactions (direct and P2P) */
+  double cell_interactions; /* Barnes-Hut multipole evaluations */
+  double cells;             /* octree cells built */
+  double eval_ms;           /* device time of the Biot-Savart kernel */
+  double build_ms;          /* device time of the tree build */
+  double total_ms;          /* device time of the whole evaluation */
+} ov_eval_stats;
+int ov_get_last_stats(ov_eval_stats *out);
+
+/* ----- device-resident state: upload once, step many times ----- */
+typedef struct ov_state ov_state;
+ov_state *ov_state_create(void);
+void ov_state_destroy(ov_state *s);
+/* copy a host tangle (positions, links, status, box, images, vels) in */
+int ov_state_upload(ov_state *s, const struct tangle_state *tangle);
+/* copy results out; what: bitmask of OV_FIELD_* */
+enum {
+  OV_FIELD_POS = 1, OV_FIELD_VELS = 2, OV_FIELD_VS = 4, OV_FIELD_TANGENTS = 8,
+  OV_FIELD_NORMALS = 16, OV_FIELD_DXI = 32, OV_FIELD_ALL = 63
+};
+int ov_state_download(ov_state *s, struct tangle_state *tangle, int what);
+/* update_tangle (tangents, normals, velocities) on the device state */
+int ov_state_update_tangle(ov_state *s, double t);
+/* rk4_step on the device state (uses its current vels as k1) */
+int ov_state_rk4_step(ov_state *s, double t, double dt);
+/* nsteps x (update_tangle + rk4_step), time advancing by dt */
+int ov_state_run(ov_state *s, double t0, double dt, int nsteps);
+/* Biot-Savart velocity (nonlocal + images, no LIA/friction) at arbitrary
+ * points from the state's current positions: method 0 = direct sum,
+ * 1 = Barnes-Hut.  pts/out: host arrays of 3*npts doubles; skip: per-point
+ * node to skip (NULL = none). */
+int ov_state_eval_points(ov_state *s, int npts, const double *pts, const int *skip,
+                         int method, double *out);
+
+/* Counters accumulated by a state since ov_state_reset_stats:
+ * evaluations, segment-point interactions (direct and Barnes-Hut leaves),
+ * multipole evaluations, device time of the Biot-Savart kernels and of the
+ * tree builds, kernel launches by this library, and the device time of the
+ * last ov_state_run (CUDA events on the state's stream). */
+typedef struct {
+  double evals;
+  double interactions;
+  double cell_interactions;
+  double bs_kernel_ms;
+  double bs_launches;
+  double build_ms;
+  double last_run_ms;
+  double launches;
+  double n_targets;
+  double n_segments;
+} ov_run_stats;
+int ov_state_get_stats(ov_state *s, ov_run_stats *out);
+void ov_state_reset_stats(ov_state *s);
+
+/* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
+ * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
+int ov_measure_fma_peak(int fp64, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPENVORT_B200_H */

@@ -1,0 +1,341 @@
+// ov_geom.cu - per-node kernels: arc lengths, 4-point tangent/normal
+// stencils, the velocity epilogue (local induction, external flow,
+// hyperfriction, mutual friction, slip) and the RK4 stage arithmetic.
+// All FP64; each thread owns one node slot.  HBM-bound: ~150 B per node.
+#include "ov_internal.h"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+struct Links {
+  const int2* lk;   // (forward, reverse) per slot
+  const int2* st;   // (status, pin_wall) per slot
+};
+
+__device__ __forceinline__ bool pinned_any(int st) { return st == OV_PINNED || st == OV_PINNED_SLIP; }
+
+// Position `where` links away from node i (step_node, src/tangle.c:165-200).
+// Walking off a pinned end continues backwards on the mirror image of the
+// vortex.  Returns false on a broken link.
+__device__ bool step_node(const OvParams& P, const Links& L, const double* pos, int i,
+                          int where, d3& out) {
+  int faces[8];
+  int nf = 0;
+  int cur = i, w = where;
+  for (int it = 0; it < 16 && w != 0; ++it) {
+    int2 st = L.st[cur];
+    bool pin = pinned_any(st.x);
+    int2 lk = L.lk[cur];
+    int nx = w > 0 ? lk.x : lk.y;
+    if (nx >= 0) {
+      cur = nx;
+      w += w > 0 ? -1 : 1;
+    } else if (pin && nf < 8) {
+      faces[nf++] = st.y;
+      w = -w;
+    } else {
+      return false;
+    }
+  }
+  if (w != 0) return false;
+  d3 p = ld3(pos, cur);
+  for (int f = nf - 1; f >= 0; --f) {
+    int face = faces[f];
+    int c = face >> 1;
+    double wp = (face & 1) ? P.hi[c] : P.lo[c];
+    set_axis(p, c, 2.0 * wp - axis_of(p, c));
+  }
+  out = p;
+  return true;
+}
+
+// Arc length `dist` links away along the stored segment lengths
+// (arc_length, src/tangle.c:208-243); reverses at a pinned end.
+__device__ bool arc_length(const Links& L, const double* dxi, int k, int dist, double& out) {
+  double acc = 0;
+  int cur = k, d = dist;
+  for (int it = 0; it < 16 && d != 0; ++it) {
+    bool pin = pinned_any(L.st[cur].x);
+    int2 lk = L.lk[cur];
+    if (d > 0) {
+      if (lk.x < 0) {
+        if (!pin) return false;
+        d = -d;
+        continue;
+      }
+      acc += dxi[cur];
+      cur = lk.x;
+      --d;
+    } else {
+      if (lk.y < 0) {
+        if (!pin) return false;
+        d = -d;
+        continue;
+      }
+      acc += dxi[lk.y];
+      cur = lk.y;
+      ++d;
+    }
+  }
+  if (d != 0) return false;
+  out = acc;
+  return true;
+}
+
+// s' and s'' at x=0 from four points p_j at arc offsets x_j: weights are the
+// first and second derivatives at 0 of the Lagrange basis through {0, x_j}
+// (the 4-point non-uniform stencils of src/tangle.c:312-344,434-470).
+__device__ void stencil4(const OvParams& P, d3 s0, const d3 p[4], const double x[4],
+                         d3& tan, d3& nrm) {
+  d3 a = mk3(0, 0, 0), b = mk3(0, 0, 0);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    double o0 = x[(j + 1) & 3], o1 = x[(j + 2) & 3], o2 = x[(j + 3) & 3];
+    double den = x[j] * (x[j] - o0) * (x[j] - o1) * (x[j] - o2);
+    double w1 = -(o0 * o1 * o2) / den;
+    double w2 = 2.0 * (o0 * o1 + o0 * o2 + o1 * o2) / den;
+    d3 d = pwrap(P, p[j], s0) - p[j];   // s0 - p_j (wrapped)
+    a = a + d * (-w1);
+    b = b + d * (-w2);
+  }
+  tan = a;
+  nrm = b;
+}
+
+__global__ void k_dxi(OvParams P, Links L, const double* __restrict__ pos, double* dxi,
+                      int n, int* flag) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  if (L.st[k].x == OV_EMPTY) return;
+  d3 s0 = ld3(pos, k), s1;
+  if (!step_node(P, L, pos, k, 1, s1)) { atomicOr(flag, 1); return; }
+  d3 w = pwrap(P, s0, s1);
+  dxi[k] = norm_ref(s0 - w);
+}
+
+// pass 0: pinned and ordinary nodes; pass 1: nodes next to a pinned node,
+// which use their neighbours' tangents (src/tangle.c:366-430)
+__global__ void k_tangents(OvParams P, Links L, const double* __restrict__ pos,
+                           const double* __restrict__ dxi, double* tan, double* nrm, int n,
+                           int pass, int* flag) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  int2 st = L.st[k];
+  if (st.x == OV_EMPTY) return;
+  int2 lk = L.lk[k];
+  bool near_pin = st.x != OV_PINNED &&
+                  ((lk.x >= 0 && L.st[lk.x].x == OV_PINNED) || (lk.y >= 0 && L.st[lk.y].x == OV_PINNED));
+  if ((pass == 1) != near_pin) return;
+  d3 s0 = ld3(pos, k), t, nn;
+  bool ok = true;
+  if (st.x == OV_PINNED) {
+    // one-sided stencil away from the wall (src/tangle.c:275-364); the
+    // reference tests forward > 0, so a forward link to slot 0 goes backwards
+    int dir = lk.x > 0 ? 1 : -1;
+    d3 p[4];
+    double x[4];
+    for (int j = 0; j < 4 && ok; ++j) {
+      double a;
+      ok = ok && arc_length(L, dxi, k, dir * (j + 1), a) && step_node(P, L, pos, k, dir * (j + 1), p[j]);
+      x[j] = dir * a;
+    }
+    if (ok) stencil4(P, s0, p, x, t, nn);
+  } else if (near_pin) {
+    d3 s1, sm1;
+    double a, bm;
+    ok = step_node(P, L, pos, k, 1, s1) && step_node(P, L, pos, k, -1, sm1) &&
+         arc_length(L, dxi, k, 1, a) && arc_length(L, dxi, k, -1, bm);
+    if (ok) {
+      double b = -bm;
+      d3 ds1 = pwrap(P, s1, s0) - s1, dsm1 = pwrap(P, sm1, s0) - sm1;
+      d3 t1 = ld3(tan, lk.x), tm1 = ld3(tan, lk.y);
+      double h = a - b, h2 = h * h, h3 = h2 * h;
+      double ct1 = -b * b / h2, ctm1 = -a * a / h2;
+      double cs1 = 2 * b * b * (b - 2 * a) / (a * h3);
+      double csm1 = 2 * a * a * (2 * b - a) / (b * h3);
+      double cn1 = 2 * b * (8 * a * a - a * b - b * b) / (a * a * h3);
+      double cnm1 = 2 * a * (a * a + a * b - 8 * b * b) / (b * b * h3);
+      double cnt1 = 2 * b * (2 * a + b) / (a * h2);
+      double cntm1 = 2 * a * (a + 2 * b) / (b * h2);
+      t = (t1 * ct1 + tm1 * ctm1) + (ds1 * cs1 + dsm1 * csm1);
+      nn = (t1 * cnt1 + tm1 * cntm1) + (ds1 * cn1 + dsm1 * cnm1);
+    }
+  } else {
+    const int off[4] = {2, 1, -1, -2};
+    d3 p[4];
+    double x[4];
+    for (int j = 0; j < 4 && ok; ++j) {
+      double a;
+      ok = ok && arc_length(L, dxi, k, off[j], a) && step_node(P, L, pos, k, off[j], p[j]);
+      x[j] = off[j] > 0 ? a : -a;
+    }
+    if (ok) stencil4(P, s0, p, x, t, nn);
+  }
+  if (!ok) { atomicOr(flag, 1); return; }
+  st3(tan, k, t);
+  st3(nrm, k, nn);
+}
+
+// velocity assembly per node (update_velocity, src/tangle.c:583-684)
+__global__ void k_epilogue(OvParams P, Links L, double t, const double* __restrict__ pos,
+                           const double* __restrict__ tan, const double* __restrict__ nrm,
+                           const double* __restrict__ v_nl, const double* __restrict__ v_img,
+                           double* vels, double* vs_out, int k0, int k1, int* flag) {
+  int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= k1) return;
+  int2 st = L.st[k];
+  if (st.x == OV_EMPTY) return;
+  d3 r = ld3(pos, k);
+  if (st.x == OV_PINNED) {
+    st3(vs_out, k, mk3(0, 0, 0));
+    st3(vels, k, flow_eval(P.vb, r, t));
+    return;
+  }
+  d3 tg = ld3(tan, k), nm = ld3(nrm, k);
+  // local induction (lia_velocity, src/tangle.c:530-551)
+  d3 nx, pv;
+  if (!step_node(P, L, pos, k, 1, nx) || !step_node(P, L, pos, k, -1, pv)) {
+    atomicOr(flag, 1);
+    return;
+  }
+  double l_next = norm_ref(r - pwrap(P, r, nx));
+  double l_prev = norm_ref(pv - pwrap(P, pv, r));
+  double f = P.kappa * log(2.0 * sqrt(l_next * l_prev) / sqrt(sqrt(OV_E)) / P.core_a) / 4.0 / OV_PI;
+  d3 lia = cross3(tg, nm) * f;
+  d3 vs = lia + flow_eval(P.vs, r, t);
+  if (!P.lia_only) {
+    vs = vs + ld3(v_nl, k);
+    if (P.n_img > 0) vs = vs + ld3(v_img, k);
+  }
+  d3 v = vs;
+  if (P.hyperfriction) {
+    if (norm_ref(nm) > P.max_curv / P.dl_max) v = v + cross3(tg, lia) * (-P.hyperalpha);
+  }
+  if (P.use_mf) {
+    d3 dv = flow_eval(P.vn, r, t) - vs;
+    v = v + cross3(tg, dv) * P.alpha;
+    v = v + cross3(tg, cross3(tg, dv)) * (-P.alpha_p);
+  }
+  if (st.x == OV_PINNED_SLIP) {
+    d3 nw = face_normal(st.y);
+    v = v - nw * dot3(nw, v);
+  }
+  if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) atomicOr(flag, 2);
+  st3(vs_out, k, vs);
+  st3(vels, k, v);
+}
+
+// x_s = x_0 + h v  (euler_step2, src/vortex_dynamics.c:36-52)
+__global__ void k_euler(const int2* __restrict__ st, const double* __restrict__ x0,
+                        const double* __restrict__ v, double h, double* xs, int n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n || st[k].x == OV_EMPTY) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) xs[3 * k + c] = x0[3 * k + c] + v[3 * k + c] * h;
+}
+
+// x += dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4 (src/vortex_dynamics.c:94-112)
+__global__ void k_rk4_combine(const int2* __restrict__ st, const double* __restrict__ k1,
+                              const double* __restrict__ k2, const double* __restrict__ k3,
+                              const double* __restrict__ k4, double dt, double* x, int n) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n || st[k].x == OV_EMPTY) return;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    int i = 3 * k + c;
+    double mv = k1[i] * (dt / 6);
+    mv += k2[i] * (dt / 3);
+    mv += k3[i] * (dt / 3);
+    mv += k4[i] * (dt / 6);
+    x[i] += mv;
+  }
+}
+
+int blocks_for(int n) { return (n + kThreads - 1) / kThreads; }
+
+}  // namespace
+
+static bool check_flag(ov_state_impl* s, const char* where) {
+  int h = 0;
+  OV_TRY_CUDA(cudaMemcpyAsync(&h, s->dflag.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  if (h & 1) {
+    ov_set_error(OV_ERR_INVALID, "%s: broken vortex links (a free node without a neighbour)", where);
+    return false;
+  }
+  if (h & 2) {
+    ov_set_error(OV_ERR_NONFINITE, "%s: non-finite velocity", where);
+    return false;
+  }
+  return true;
+}
+
+bool ov_geometry(ov_state_impl* s, const double* pos, double* dxi, double* tan, double* nrm) {
+  if (s->n == 0) return true;
+  Links L{s->links.as<int2>(), s->status.as<int2>()};
+  int* flag = s->dflag.as<int>();
+  OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+  k_dxi<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->P, L, pos, dxi, s->n, flag);
+  OV_LAUNCHED();
+  k_tangents<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->P, L, pos, dxi, tan, nrm, s->n, 0, flag);
+  OV_LAUNCHED();
+  k_tangents<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->P, L, pos, dxi, tan, nrm, s->n, 1, flag);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return check_flag(s, "update_tangents_normals");
+}
+
+bool ov_epilogue(ov_state_impl* s, double t, const double* pos, const double* tan,
+                 const double* nrm, const double* v_nl, const double* v_img, double* vels,
+                 double* vs, int k0, int k1) {
+  if (k1 <= k0) return true;
+  Links L{s->links.as<int2>(), s->status.as<int2>()};
+  int* flag = s->dflag.as<int>();
+  OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+  k_epilogue<<<blocks_for(k1 - k0), kThreads, 0, s->stream>>>(s->P, L, t, pos, tan, nrm, v_nl, v_img,
+                                                              vels, vs, k0, k1, flag);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return check_flag(s, "update_velocities");
+}
+
+bool ov_euler(ov_state_impl* s, double dt) {
+  if (s->n == 0) return true;
+  k_euler<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->status.as<int2>(), s->pos.as<double>(),
+                                                         s->vels.as<double>(), dt,
+                                                         s->pos.as<double>(), s->n);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+// rk4_step2 (src/vortex_dynamics.c:58-117) on the device state.  Stage 4
+// advances dt/2 like the reference unless `classic`.
+bool ov_rk4(ov_state_impl* s, double t, double dt, int classic) {
+  if (s->n == 0) return true;
+  const int2* st = s->status.as<int2>();
+  double* x0 = s->pos.as<double>();
+  double* xs = s->spos.as<double>();
+  double* ks[3] = {s->k2.as<double>(), s->k3.as<double>(), s->k4.as<double>()};
+  const double h[3] = {dt / 2, dt / 2, classic ? dt : dt / 2};
+  const double ts[3] = {t + dt / 2, t + dt / 2, t + dt};
+  // EMPTY slots of the stage positions are never read, but keep them defined
+  OV_TRY_CUDA(cudaMemcpyAsync(xs, x0, sizeof(double) * 3 * s->n, cudaMemcpyDeviceToDevice, s->stream));
+  for (int q = 0; q < 3; ++q) {
+    const double* prev = q == 0 ? s->vels.as<double>() : ks[q - 1];
+    k_euler<<<blocks_for(s->n), kThreads, 0, s->stream>>>(st, x0, prev, h[q], xs, s->n);
+    OV_LAUNCHED();
+    OV_TRY_CUDA(cudaGetLastError());
+    if (!ov_geometry(s, xs, s->sdxi.as<double>(), s->stan.as<double>(), s->snrm.as<double>()))
+      return false;
+    if (!ov_velocities(s, ts[q], xs, s->sdxi.as<double>(), s->stan.as<double>(),
+                       s->snrm.as<double>(), ks[q], s->svs.as<double>(), nullptr))
+      return false;
+  }
+  k_rk4_combine<<<blocks_for(s->n), kThreads, 0, s->stream>>>(st, s->vels.as<double>(), ks[0], ks[1],
+                                                               ks[2], dt, x0, s->n);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}

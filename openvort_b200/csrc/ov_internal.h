@@ -1,0 +1,161 @@
+// ov_internal.h - host-side internals shared by the translation units of
+// libov_gpu.so: the device state behind ov_state, the Barnes-Hut tree, the
+// error channel and the kernel launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "openvort_b200.h"
+#include "ov_device.cuh"
+
+// ---------------------------------------------------------------- errors
+void ov_set_error(int code, const char* fmt, ...);
+bool ov_cuda_ok(cudaError_t e, const char* what);
+#define OV_TRY_CUDA(expr)                          \
+  do {                                             \
+    if (!ov_cuda_ok((expr), #expr)) return false;  \
+  } while (0)
+
+// ---------------------------------------------------------------- buffers
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool reserve(size_t n);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+// ---------------------------------------------------------------- BH tree
+// Octree cell kinds (what the walk does with a cell it reaches):
+//   CELL_LEAF     : N == 1, or the cell's box is below BH_grain: direct sum
+//                   over the cell's nodes, no opening test
+//   CELL_OPEN     : opening test; on failure descend into the children
+//   CELL_OPEN_P2P : opening test; on failure direct sum over the cell's nodes
+//                   (a chain of single-child cells ending in a grain leaf)
+//   CELL_OPEN_ZERO: opening test; on failure nothing (unsplit or all nodes
+//                   dropped from the children, src/octree.c:104,118-127)
+enum { CELL_LEAF = 0, CELL_OPEN = 1, CELL_OPEN_P2P = 2, CELL_OPEN_ZERO = 3 };
+
+// One cell in depth-first preorder.  Children of cell c start at c + 1;
+// the first cell after c's subtree is `skip`.
+struct __align__(16) CellMeta {
+  int start;   // first node (sorted order)
+  int count;   // nodes in the cell (including nodes dropped deeper down)
+  int skip;    // preorder index after this cell's subtree
+  int kind;    // CELL_*
+  double thr;  // opening test passes iff |r - com|^2 (reference wrapping) >= thr
+  double Lm;   // max box size at the tested level (for user-supplied theta)
+};
+
+struct __align__(16) CellMom64 {  // kappa/4pi-scaled moments, FP64
+  double com[3];
+  double gam[3];                  // sum of segment vectors
+  double m21, m02, m12, m22;      // the circulation-tensor entries the expansion uses
+};
+
+struct __align__(16) CellMom32 {  // FP32 copy of the scaled moments
+  float gam[3];
+  float m21, m02, m12, m22;
+  float pad;
+};
+
+struct OvTree {
+  int n_nodes = 0;      // active (non-EMPTY) nodes
+  int n_cells = 0;
+  int built = 0;
+  double theta = 0;     // theta used for thr
+  OvParams P;           // parameters at build time
+  DevBuf keys, keys_alt, vals, vals_alt, stop, hist;   // sort
+  DevBuf perm;          // sorted index -> slot
+  DevBuf bnode;         // binary radix tree nodes
+  DevBuf cstart_cnt, cbase, cell_of;   // preorder bookkeeping
+  DevBuf meta, mom64, mom32;           // cells
+  DevBuf nodes64;       // per sorted node: r1 (3), r2 wrapped (3)
+  DevBuf nodeids;       // per sorted node: slot, forward slot
+  DevBuf nodes32;       // per sorted node: r1 - cell-free origin (FP32 not used yet)
+  DevBuf counters;      // device counters (interactions, cells visited)
+  DevBuf scratch;
+};
+
+// ---------------------------------------------------------------- state
+struct ov_state_impl {
+  int cap = 0;          // slot capacity of the device arrays
+  int n = 0;            // slots in use
+  OvParams P;           // captured at upload / call time
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr;
+  // slot-indexed (AoS, 3 doubles per vector, as struct vec3d)
+  DevBuf pos, links, status, dxi, tan, nrm, vels, vs;
+  // RK4 scratch
+  DevBuf pos0, spos, sdxi, stan, snrm, svs, k2, k3, k4;
+  // Biot-Savart outputs: primary sum and image sum per slot
+  DevBuf v_nl, v_img;
+  // direct-sum per-image partials and segment table
+  DevBuf img_part, seg64, segid;
+  // error flag written by kernels (bounded waits, broken links)
+  DevBuf dflag;
+  OvTree tree;
+  double t_last = 0;
+  // accumulated over evaluations since the last reset (ov_state_get_stats)
+  double acc_evals = 0, acc_inter = 0, acc_cells = 0, acc_bs_ms = 0, acc_bs_launches = 0;
+  double acc_build_ms = 0, last_run_ms = 0;
+  long long launches_at_reset = 0;
+  int n_targets = 0, n_segments = 0;
+  cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+};
+
+// ---------------------------------------------------------------- launchers
+// geometry: dxi, tangents, normals of all slots (pos/links/status -> dxi,tan,nrm)
+bool ov_geometry(ov_state_impl* s, const double* pos, double* dxi, double* tan, double* nrm);
+// velocities at positions pos with tangents/normals -> vels, vs
+bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* dxi,
+                   const double* tan, const double* nrm, double* vels, double* vs,
+                   OvTree* external_tree);
+// one RK4 step on the state's pos using the state's vels as k1
+bool ov_rk4(ov_state_impl* s, double t, double dt, int classic);
+bool ov_euler(ov_state_impl* s, double dt);
+
+// tree over the positions pos (slot-indexed); fills tree
+bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* tree);
+void ov_tree_release(OvTree* tree);
+// Barnes-Hut nonlocal + image sums for every active node -> v_nl, v_img
+// own_tree: the tree was built from `pos` (targets in its key order)
+bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* tree, const double* pos, bool own_tree,
+                        double* v_nl, double* v_img);
+// Barnes-Hut sums at arbitrary points (device arrays): out_nl = the tangle's
+// own sum (skip per point), out_img = the image sum (nullptr: no images)
+bool ov_tree_walk_points(ov_state_impl* s, OvTree* tree, int npts, const double* pts,
+                         const int* skip, double theta, double* out_nl, double* out_img);
+
+// direct sums for all nodes -> v_nl, v_img
+bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* v_img);
+// direct sums at arbitrary points (device arrays), sources = all segments or
+// the slot list `only`: out_nl = the tangle's own sum, out_img = image sum
+// (nullptr: no images)
+bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const double* pts,
+                      const int* skip, const int* only, int n_only, double* out_nl,
+                      double* out_img);
+// out = a + b for n vectors of 3 doubles (device)
+bool ov_add3(cudaStream_t st, const double* a, const double* b, double* out, int n);
+
+// epilogue: LIA + external + v_nl + v_img + hyperfriction + mutual friction
+// for slots k0 <= k < k1
+bool ov_epilogue(ov_state_impl* s, double t, const double* pos, const double* tan,
+                 const double* nrm, const double* v_nl, const double* v_img,
+                 double* vels, double* vs, int k0, int k1);
+
+bool ov_state_reserve(ov_state_impl* s, int n);
+
+// per-thread statistics of the last evaluation
+struct OvStatsAcc {
+  double interactions, cell_interactions, cells, eval_ms, build_ms, total_ms;
+};
+OvStatsAcc& ov_stats_tls();
+
+// kernel launches issued by this library (all threads)
+void ov_note_launch(int n);
+long long ov_launches();
+#define OV_LAUNCHED() ov_note_launch(1)

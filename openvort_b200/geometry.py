@@ -1,0 +1,148 @@
+"""Seeded tangle generators for the benchmark and test workloads.
+
+Rings are placed with the reference's circle geometry (add_circle,
+src/vortex_utils.c:52-99), so the CPU reference and the GPU receive identical
+positions and links.  All randomness comes from numpy's default_rng(seed).
+"""
+from __future__ import annotations
+
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from .tangle import EMPTY, FREE, HostTangle, ring_points
+
+
+def rings_to_tangle(rings: Sequence[np.ndarray], box_lo, box_hi, boundary: str,
+                    wrap: bool = False, empty_slots: int = 0, alloc=np.empty) -> HostTangle:
+    """Concatenate closed loops (each an (n, 3) array in order) into one
+    tangle: node i of a loop links forward to i+1 and back to i-1."""
+    pos, fwd, rev = [], [], []
+    off = 0
+    for r in rings:
+        n = len(r)
+        idx = np.arange(n)
+        pos.append(r)
+        fwd.append(off + (idx + 1) % n)
+        rev.append(off + (idx - 1) % n)
+        off += n
+    pos = np.concatenate(pos) if pos else np.zeros((0, 3))
+    fwd = np.concatenate(fwd).astype(np.int32) if fwd else np.zeros(0, np.int32)
+    rev = np.concatenate(rev).astype(np.int32) if rev else np.zeros(0, np.int32)
+    status = np.full(len(pos), FREE, np.int32)
+    if wrap:
+        lo = np.asarray(box_lo, dtype=np.float64)
+        L = np.asarray(box_hi, dtype=np.float64) - lo
+        pos = lo + np.mod(pos - lo, L)
+    if empty_slots:
+        # EMPTY holes interleaved with the nodes, as remeshing leaves them
+        n = len(pos)
+        total = n + empty_slots
+        rng = np.random.default_rng(12345)
+        holes = np.sort(rng.choice(total, size=empty_slots, replace=False))
+        keep = np.setdiff1d(np.arange(total), holes)
+        newpos = np.zeros((total, 3))
+        newpos[keep] = pos
+        newpos[holes] = 0.5 * (np.asarray(box_lo) + np.asarray(box_hi))
+        remap = np.full(n, -1, np.int64)
+        remap[np.arange(n)] = keep
+        nf = np.full(total, -1, np.int32)
+        nr = np.full(total, -1, np.int32)
+        nf[keep] = remap[fwd]
+        nr[keep] = remap[rev]
+        st = np.full(total, EMPTY, np.int32)
+        st[keep] = FREE
+        pos, fwd, rev, status = newpos, nf, nr, st
+    return HostTangle(pos, fwd, rev, status, None, box_lo, box_hi, boundary, alloc=alloc)
+
+
+def single_ring(n: int = 256, radius: float = 1e-2, center=(0.0, 0.0, 0.0),
+                direction=(0.0, 0.0, 1.0), box_half: float = 0.05, alloc=np.empty) -> HostTangle:
+    """One circular ring in open space; the box encloses it (the box only
+    matters to the Barnes-Hut tree, src/tangle.c:102-105)."""
+    c = np.asarray(center, dtype=np.float64)
+    r = ring_points(c, direction, radius, n)
+    return rings_to_tangle([r], c - box_half, c + box_half, "open", alloc=alloc)
+
+
+def random_ring_tangle(seed: int, n_rings: int, D: float, r_frac=(0.02, 0.05), dl=None,
+                       boundary: str = "periodic-26", empty_slots: int = 0,
+                       alloc=np.empty) -> HostTangle:
+    """Rings with centres uniform in [0, D]^3, normals uniform on the sphere,
+    radii uniform in [r_frac] * D, about 2 pi r / dl points each; positions
+    wrapped into the periodic box."""
+    rng = np.random.default_rng(seed)
+    dl = D / 200 if dl is None else dl
+    rings = []
+    for _ in range(n_rings):
+        c = rng.uniform(0.0, D, size=3)
+        d = rng.normal(size=3)
+        d /= np.sqrt(d @ d)
+        r = rng.uniform(r_frac[0] * D, r_frac[1] * D)
+        n = max(5, int(round(2 * np.pi * r / dl)))
+        rings.append(ring_points(c, d, r, n))
+    return rings_to_tangle(rings, (0.0, 0.0, 0.0), (D, D, D), boundary, wrap=True,
+                           empty_slots=empty_slots, alloc=alloc)
+
+
+def rings_for_points(target_points: int, D: float, r_frac=(0.02, 0.05), dl=None) -> int:
+    """Number of rings whose expected point count is target_points."""
+    dl = D / 200 if dl is None else dl
+    mean_n = 2 * np.pi * 0.5 * (r_frac[0] + r_frac[1]) * D / dl
+    return max(1, int(round(target_points / mean_n)))
+
+
+def ring_pair_system(rng: np.random.Generator, kind: str, n_total: int,
+                     r_range=(5e-3, 2e-2)) -> List[np.ndarray]:
+    """Two rings on the z axis: 'leapfrog' (same direction) or 'headon'
+    (opposite directions), radii uniform in r_range, points split by length."""
+    r1, r2 = rng.uniform(*r_range, size=2)
+    n1 = max(8, int(round(n_total * r1 / (r1 + r2))))
+    n2 = max(8, n_total - n1)
+    gap = 0.5 * (r1 + r2)
+    if kind == "leapfrog":
+        a = ring_points((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), r1, n1)
+        b = ring_points((0.0, 0.0, gap), (0.0, 0.0, 1.0), r2, n2)
+    else:
+        a = ring_points((0.0, 0.0, -gap), (0.0, 0.0, 1.0), r1, n1)
+        b = ring_points((0.0, 0.0, gap), (0.0, 0.0, -1.0), r2, n2)
+    return [a, b]
+
+
+def kelvin_ring(seed: int, n: int = 4096, radius: float = 1e-2, modes=(2, 32),
+                sigma: float = 1e-4) -> np.ndarray:
+    """A ring with a seeded Kelvin-wave perturbation: radial and axial
+    displacements sum_m a_m cos(m phi + phase_m), amplitudes N(0, sigma^2)."""
+    rng = np.random.default_rng(seed)
+    base = ring_points((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), radius, n)
+    phi = 2 * np.pi * np.arange(n) / n
+    dr = np.zeros(n)
+    dz = np.zeros(n)
+    for m in range(modes[0], modes[1] + 1):
+        a, b = rng.normal(0.0, sigma, size=2)
+        p1, p2 = rng.uniform(0, 2 * np.pi, size=2)
+        dr += a * np.cos(m * phi + p1)
+        dz += b * np.cos(m * phi + p2)
+    rad = base[:, :2] / np.linalg.norm(base[:, :2], axis=1)[:, None]
+    out = base.copy()
+    out[:, :2] += rad * dr[:, None]
+    out[:, 2] += dz
+    return out
+
+
+def wall_half_ring(n: int = 64, radius: float = 1e-2, box=0.05) -> HostTangle:
+    """A half ring standing on the z = 0 mirror wall with both ends pinned
+    (pinned one-sided stencils, mirror image, boundary velocity)."""
+    phi = np.linspace(0.0, np.pi, n)
+    pos = np.stack([radius * np.cos(phi), np.zeros(n), radius * np.sin(phi)], axis=1)
+    pos[0, 2] = 0.0
+    pos[-1, 2] = 0.0
+    idx = np.arange(n)
+    fwd = np.where(idx < n - 1, idx + 1, -1).astype(np.int32)
+    rev = np.where(idx > 0, idx - 1, -1).astype(np.int32)
+    status = np.full(n, FREE, np.int32)
+    status[0] = status[-1] = 1  # PINNED
+    pin = np.full(n, -1, np.int32)
+    pin[0] = pin[-1] = 4        # Z_L
+    return HostTangle(pos, fwd, rev, status, pin, (-box, -box, 0.0), (box, box, 2 * box),
+                      "wall-1-open")

@@ -1,0 +1,95 @@
+"""Generate the golden fixtures in tests/golden/*.npz from the UNMODIFIED
+OpenVort reference (oracle/_ref/libov_ref.so, compiled from the reference's
+own sources by oracle/Makefile).
+
+    python tests/golden/make_golden.py
+
+Each fixture holds a seeded input tangle (positions, links, status, box,
+boundary name), the run-time parameters, and the reference's outputs:
+dxi, tangents, normals, vels, vs after update_tangle, and for the RK4 cases
+the positions after a number of rk4_step calls (update_tangle before each,
+as the reference's main loop does, src/main.c:112-114).
+"""
+from __future__ import annotations
+
+import json
+import sys
+from dataclasses import asdict
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from openvort_b200 import geometry as G  # noqa: E402
+from openvort_b200.tangle import Flow, Params  # noqa: E402
+from oracle.oracle import Ref, build  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def params_json(p: Params) -> str:
+    d = asdict(p)
+    return json.dumps(d)
+
+
+def cases():
+    ring_p = Params(core_a=1.3e-8, use_mf=0, alpha=0.0, alpha_p=0.0, hyperfriction=0,
+                    dl_max=2 * 2 * np.pi * 1e-2 / 256)
+    yield "ring256", G.single_ring(256, 1e-2), ring_p, {"rk4_steps": 10, "dt": 5e-6}
+    per_p = Params(core_a=1.3e-8, alpha=0.098, alpha_p=0.016, dl_max=2 * 0.1 / 200,
+                   vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}))
+    t = G.random_ring_tangle(1, 20, 0.1, boundary="periodic-26")
+    yield "periodic26_direct", t, per_p, {"rk4_steps": 2, "dt": 1e-6}
+    for th in (0.3, 0.4, 0.5):
+        p = Params(**{**per_p.__dict__, "use_bh": 1, "bh_theta": th})
+        yield f"periodic26_bh{int(th * 10)}", t, p, {"rk4_steps": 1 if th == 0.4 else 0, "dt": 1e-6}
+    # open boundaries, EMPTY holes between the nodes, hyperfriction on
+    t2 = G.random_ring_tangle(2, 8, 0.1, boundary="open", empty_slots=17)
+    t2.box_lo, t2.box_hi = (-0.05,) * 3, (0.15,) * 3
+    t2._bind()
+    p2 = Params(core_a=1.3e-8, alpha=0.1, alpha_p=0.01, dl_max=1e-3, hyperfriction=1,
+                max_curv_scale=0.2, vn=Flow("simple", {"external_v": (0.0, 0.3, 0.0)}),
+                vs=Flow("simple", {"external_v": (0.01, 0.0, 0.0)}))
+    yield "open_empty_direct", t2, p2, {"rk4_steps": 1, "dt": 1e-6}
+    yield "open_empty_bh4", t2, Params(**{**p2.__dict__, "use_bh": 1, "bh_theta": 0.4}), {"rk4_steps": 0, "dt": 0}
+    # a half ring pinned on a mirror wall: pinned stencils, mirror image, v_b
+    w = G.wall_half_ring(64)
+    pw = Params(core_a=1.3e-8, dl_max=2e-3, hyperfriction=0, alpha=0.05, alpha_p=0.01,
+                vn=Flow("coscos", {"k": 50.0, "v0": 0.1, "l": 0.05}),
+                vb=Flow("no flow"))
+    yield "wall_half_ring", w, pw, {"rk4_steps": 0, "dt": 0}
+    # periodic-z image table with a time-dependent flow
+    t3 = G.random_ring_tangle(4, 6, 0.1, boundary="periodic-z-open-xy")
+    p3 = Params(core_a=1e-8, alpha=0.1, alpha_p=0.02, dl_max=1e-3,
+                vn=Flow("oscillating", {"strength": 0.3, "frequency": 50.0,
+                                        "wave": (10.0, 0.0, 5.0), "polarization": (0.0, 1.0, 0.0)}),
+                vs=Flow("rotosc", {"freq": 20.0, "amp": 0.5}))
+    yield "periodic_z_flows", t3, p3, {"rk4_steps": 1, "dt": 1e-6, "time": 0.003}
+
+
+def main():
+    build()
+    ref = Ref(threads=8)
+    for name, t, p, opt in cases():
+        time = opt.get("time", 0.0)
+        u = ref.update_tangle(t, p, time)
+        arrays = dict(pos=t.pos, fwd=t.links[:, 0], rev=t.links[:, 1], status=t.stat[:, 0],
+                      pin_wall=t.stat[:, 1], box_lo=np.array(t.box_lo), box_hi=np.array(t.box_hi),
+                      dxi=u.dxi, tangents=u.tangents, normals=u.normals, vels=u.vels, vs=u.vs)
+        meta = {"boundary": t.boundary, "params": json.loads(params_json(p)), "time": time,
+                "rk4_steps": opt["rk4_steps"], "dt": opt["dt"]}
+        cur = u
+        tt = time
+        for s in range(opt["rk4_steps"]):
+            nxt = ref.rk4_step(cur, p, tt, opt["dt"])
+            tt += opt["dt"]
+            cur = ref.update_tangle(nxt, p, tt)
+            arrays[f"rk4_pos_{s + 1}"] = cur.pos
+        np.savez_compressed(OUT / f"{name}.npz", meta=np.array(json.dumps(meta)), **arrays)
+        print(name, t.n, "nodes")
+
+
+if __name__ == "__main__":
+    main()

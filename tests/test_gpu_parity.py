@@ -1,0 +1,269 @@
+"""GPU parity: libov_gpu.so, called through its C ABI (the reference-named
+entry points and ov_state_*), against the reference's golden fixtures and the
+CPU oracle on the same seeded inputs.
+
+Tolerances (max over nodes of |dv| / |v_ref|):
+  FP64 path   1e-12 on velocities (tangents 1e-11, normals 1e-10: second
+              differences of positions ~dl apart lose ~3 digits, and the
+              stencil weights are factored differently from the reference)
+  mixed path  1e-5 on velocities
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from cases import NAMES, load, pos_err, rel_err
+from openvort_b200 import geometry as G
+from openvort_b200.tangle import Flow, Params, Vec3d
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_V64, TOL_T64, TOL_N64, TOL_MIXED = 1e-12, 1e-11, 1e-10, 1e-5
+
+
+@pytest.fixture(scope="module")
+def ov():
+    import openvort_b200 as ov
+    lib = ov.load()
+    assert lib.ov_init(0) == 0, lib.ov_last_error_message()
+    return ov
+
+
+@pytest.fixture(scope="module")
+def oracle():
+    return Oracle()
+
+
+def gpu_update(ov, t, p, time=0.0, precision=0):
+    ov.configure(p, precision)
+    out = t.copy()
+    ov.update_tangle(out, time)
+    return out
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_update_tangle_fp64_vs_golden(ov, name):
+    t, p, meta, z = load(name)
+    out = gpu_update(ov, t, p, meta["time"])
+    act = t.active
+    assert np.max(np.abs(out.dxi - z["dxi"])[act]) <= 1e-15 * np.max(z["dxi"][act])
+    assert rel_err(out.tangents, z["tangents"], act) < TOL_T64
+    assert rel_err(out.normals, z["normals"], act) < TOL_N64
+    assert rel_err(out.vs, z["vs"], act) < TOL_V64
+    assert rel_err(out.vels, z["vels"], act) < TOL_V64
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_update_tangle_mixed_vs_golden(ov, name):
+    t, p, meta, z = load(name)
+    out = gpu_update(ov, t, p, meta["time"], precision=1)
+    assert rel_err(out.vels, z["vels"], t.active) < TOL_MIXED
+
+
+@pytest.mark.parametrize("name", [n for n in NAMES if n in ("ring256", "periodic26_direct",
+                                                           "periodic26_bh4", "open_empty_direct",
+                                                           "periodic_z_flows")])
+def test_rk4_fp64_vs_golden(ov, name):
+    t, p, meta, z = load(name)
+    ov.configure(p, 0)
+    cur = t.copy()
+    tt = meta["time"]
+    ov.update_tangle(cur, tt)
+    for s in range(meta["rk4_steps"]):
+        ov.rk4_step(cur, tt, meta["dt"])
+        tt += meta["dt"]
+        ov.update_tangle(cur, tt)
+        assert pos_err(cur.pos, z[f"rk4_pos_{s + 1}"], t.active) < 1e-14
+
+
+def test_device_state_run_vs_oracle(ov, oracle):
+    """ov_state_run (device-resident update_tangle + rk4_step) against the
+    oracle stepping the same tangle on the CPU."""
+    t, p, meta, z = load("periodic26_bh4")
+    ov.configure(p, 0)
+    st = ov.DeviceState(t.copy())
+    st.run(0.0, 1e-6, 3)
+    st.download()
+    cur = oracle.update_tangle(t, p, 0.0)
+    tt = 0.0
+    for _ in range(3):
+        nxt = oracle.rk4_step(cur, p, tt, 1e-6)
+        tt += 1e-6
+        cur = oracle.update_tangle(nxt, p, tt)
+    assert pos_err(st.t.pos, cur.pos, t.active) < 1e-14
+    st.close()
+
+
+@pytest.mark.parametrize("theta", [0.3, 0.5])
+def test_bh_larger_tangle_vs_oracle(ov, oracle, theta):
+    """~4k nodes, periodic-26, both precisions against the FP64 oracle."""
+    t = G.random_ring_tangle(3, 100, 0.1, boundary="periodic-26", empty_slots=9)
+    p = Params(core_a=1.3e-8, alpha=0.098, alpha_p=0.016, dl_max=1e-3, use_bh=1, bh_theta=theta,
+               vn=Flow("simple", {"external_v": (0.5, 0, 0)}))
+    ref = oracle.update_tangle(t, p)
+    g64 = gpu_update(ov, t, p)
+    assert rel_err(g64.vels, ref.vels, t.active) < TOL_V64
+    gmx = gpu_update(ov, t, p, precision=1)
+    assert rel_err(gmx.vels, ref.vels, t.active) < TOL_MIXED
+
+
+def test_quadtree_vs_oracle(ov, oracle):
+    t = G.random_ring_tangle(8, 30, 0.1, boundary="periodic-6")
+    p = Params(core_a=1.3e-8, alpha=0.1, alpha_p=0.01, dl_max=1e-3, use_bh=1, bh_theta=0.4,
+               bh_quadtree=1)
+    assert rel_err(gpu_update(ov, t, p).vels, oracle.update_tangle(t, p).vels, t.active) < TOL_V64
+
+
+def test_point_queries(ov, oracle):
+    """calculate_vs / calculate_vs_shift / octree_get_vs at arbitrary points."""
+    t, p, _, _ = load("periodic26_bh4")
+    lib = ov.load()
+    ov.configure(p, 0)
+    t.set_images_from_library(lib)
+    rng = np.random.default_rng(7)
+    pts = rng.uniform(0, 0.1, size=(8, 3))
+    skip = [-1, 3, 10, -1, 50, 7, -1, 0]
+    want = oracle.segments_at(t, p, pts, np.array(skip, np.int32))
+    for i in range(8):
+        v = lib.calculate_vs(t.ptr(), Vec3d((C.c_double * 3)(*pts[i])), skip[i])
+        ov.check(lib)
+        assert rel_err(np.array(v.p)[None], want[i:i + 1]) < TOL_V64
+    # calculate_vs_shift with a node list and a shift
+    only = np.arange(0, t.n, 3, dtype=np.int32)
+    sh = Vec3d((C.c_double * 3)(0.01, -0.02, 0.005))
+    v = lib.calculate_vs_shift(t.ptr(), Vec3d((C.c_double * 3)(*pts[0])), -1, C.byref(sh),
+                               only.ctypes.data_as(C.POINTER(C.c_int)), len(only))
+    ov.check(lib)
+    sub = t.copy()
+    sub.links[np.setdiff1d(np.arange(t.n), only), 0] = -1
+    w = oracle.segments_at(sub, p, pts[:1] + np.array([0.01, -0.02, 0.005]))
+    assert rel_err(np.array(v.p)[None], w) < TOL_V64
+    # octree_build / octree_get_vs (no images), at the build theta and another
+    tree = lib.octree_build(t.ptr(), 0)
+    ov.check(lib)
+    want = oracle.bh_at(t, p, pts, np.array(skip, np.int32))
+    for i in range(8):
+        res = Vec3d()
+        lib.octree_get_vs(tree, C.byref(Vec3d((C.c_double * 3)(*pts[i]))), p.bh_theta, C.byref(res), skip[i])
+        ov.check(lib)
+        assert rel_err(np.array(res.p)[None], want[i:i + 1]) < TOL_V64
+    p2 = Params(**{**p.__dict__, "bh_theta": 0.25})
+    want2 = oracle.bh_at(t, p2, pts[:2])
+    for i in range(2):
+        res = Vec3d()
+        lib.octree_get_vs(tree, C.byref(Vec3d((C.c_double * 3)(*pts[i]))), 0.25, C.byref(res), -1)
+        assert rel_err(np.array(res.p)[None], want2[i:i + 1]) < TOL_V64
+    lib.octree_destroy(tree)
+
+
+def test_update_velocity_single_node(ov):
+    """update_velocity(k) (the reference's reconnection calls it per node)
+    equals node k of update_velocities, direct and with a tree."""
+    for name in ("periodic26_direct", "periodic26_bh4"):
+        t, p, meta, z = load(name)
+        lib = ov.load()
+        ov.configure(p, 0)
+        cur = t.copy()
+        cur.tangents[:] = z["tangents"]
+        cur.normals[:] = z["normals"]
+        cur.set_images_from_library(lib)
+        tree = lib.octree_build(cur.ptr(), 0) if p.use_bh else None
+        for k in (0, 17, 400, t.n - 1):
+            cur.vels[k] = 0
+            lib.update_velocity(cur.ptr(), k, 0.0, tree)
+            ov.check(lib)
+            assert rel_err(cur.vels[k:k + 1], z["vels"][k:k + 1]) < TOL_V64
+        if tree:
+            lib.octree_destroy(tree)
+
+
+def test_update_velocities_with_user_tree(ov):
+    t, p, meta, z = load("periodic26_bh3")
+    lib = ov.load()
+    ov.configure(p, 0)
+    cur = t.copy()
+    cur.tangents[:] = z["tangents"]
+    cur.normals[:] = z["normals"]
+    cur.set_images_from_library(lib)
+    tree = lib.octree_build(cur.ptr(), 0)
+    lib.update_velocities(cur.ptr(), 0.0, tree)
+    ov.check(lib)
+    lib.octree_destroy(tree)
+    assert rel_err(cur.vels, z["vels"], t.active) < TOL_V64
+
+
+def test_eval_points_direct_and_bh(ov, oracle):
+    t, p, _, _ = load("periodic26_bh5")
+    ov.configure(p, 0)
+    st = ov.DeviceState(t.copy())
+    rng = np.random.default_rng(9)
+    pts = rng.uniform(0, 0.1, size=(100, 3))
+    d = st.eval_points(pts, method=0)
+    # direct with images at points = the tangle's own sum + image sum
+    ref = oracle.segments_at(t, p, pts)
+    L = 0.1
+    from openvort_b200.tangle import IMAGE_TABLES
+    for sh, _ in IMAGE_TABLES["periodic-26"]:
+        ref = ref + oracle.segments_at(t, p, pts - L * np.array(sh))
+    assert rel_err(d, ref) < TOL_V64
+    b = st.eval_points(pts, method=1)
+    assert 1e-6 < rel_err(b, ref) < 0.5
+    st.close()
+
+
+def test_ring_speed_thin_core_gpu(ov, oracle):
+    """1000 RK4 steps of the 256-point ring (dt 5e-6): mean speed within 3 %
+    of kappa/(4 pi R)(ln(8R/a) - 1/2) and equal to the oracle's first step."""
+    R, a, kappa = 1e-2, 1.3e-8, 9.97e-4
+    t = G.single_ring(256, R)
+    p = Params(core_a=a, use_mf=0, alpha=0, alpha_p=0, hyperfriction=0, dl_max=2 * 2 * np.pi * R / 256)
+    ov.configure(p, 0)
+    st = ov.DeviceState(t.copy())
+    z0 = t.pos[:, 2].mean()
+    st.run(0.0, 5e-6, 1000)
+    st.download()
+    v = (st.t.pos[:, 2].mean() - z0) / (1000 * 5e-6)
+    v_thin = kappa / (4 * np.pi * R) * (np.log(8 * R / a) - 0.5)
+    assert abs(v / v_thin - 1) < 0.03
+    # radius conserved to the discretisation
+    c = st.t.pos.mean(axis=0)
+    rr = np.linalg.norm(st.t.pos - c, axis=1)
+    assert np.max(np.abs(rr / R - 1)) < 1e-3
+    st.close()
+
+
+def test_broken_links_fail_loudly(ov, monkeypatch):
+    monkeypatch.setenv("OV_QUIET", "1")
+    t = G.single_ring(32, 1e-2)
+    t.links[5, 0] = -1   # a FREE node with no forward neighbour
+    ov.configure(Params(use_mf=0, hyperfriction=0), 0)
+    with pytest.raises(ov.OVError) as e:
+        ov.update_tangents_normals(t)
+    assert e.value.code == 3
+
+
+def test_unknown_flow_fails_loudly(ov, monkeypatch):
+    monkeypatch.setenv("OV_QUIET", "1")
+    t = G.single_ring(32, 1e-2)
+    p = Params(use_mf=1, hyperfriction=0, vn=Flow("simple", {"external_v": (1, 0, 0)}))
+    lib = ov.configure(p, 0)
+    conf, keep = Flow("simple").vconf()
+    conf.name = b"no such flow"
+    C.memmove(C.addressof(type(conf).in_dll(lib, "vn_conf")), C.addressof(conf), C.sizeof(conf))
+    with pytest.raises(ov.OVError) as e:
+        ov.update_tangle(t, 0.0)
+    assert e.value.code == 5
+
+
+def test_mixed_vs_fp64_large_bh(ov):
+    """Size-independent property at ~200k nodes: the mixed form stays within
+    1e-5 of the FP64 form on the same tree and theta."""
+    t = G.random_ring_tangle(21, G.rings_for_points(200_000, 0.2, dl=0.2 / 400), 0.2,
+                             dl=0.2 / 400, boundary="periodic-26")
+    p = Params(core_a=1.3e-8, alpha=0.098, alpha_p=0.016, dl_max=2 * 0.2 / 400, use_bh=1,
+               bh_theta=0.5, vn=Flow("simple", {"external_v": (0.5, 0, 0)}))
+    a = gpu_update(ov, t, p, precision=0)
+    b = gpu_update(ov, t, p, precision=1)
+    assert rel_err(b.vels, a.vels, t.active) < TOL_MIXED
