@@ -282,6 +282,7 @@ typedef struct {
   double launches;
   double n_targets;
   double n_segments;
+  double warp_iterations;   /* Barnes-Hut walk: cells visited per warp, summed */
 } ov_run_stats;
 int ov_state_get_stats(ov_state *s, ov_run_stats *out);
 void ov_state_reset_stats(ov_state *s);

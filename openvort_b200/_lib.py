@@ -55,7 +55,8 @@ class EvalStats(C.Structure):
 class RunStats(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("evals", "interactions", "cell_interactions",
                                           "bs_kernel_ms", "bs_launches", "build_ms",
-                                          "last_run_ms", "launches", "n_targets", "n_segments")]
+                                          "last_run_ms", "launches", "n_targets", "n_segments",
+                                          "warp_iterations")]
 
 
 _lib = None

@@ -123,7 +123,7 @@ const struct boundary_images channel_z = {t_channel_z, 6};
 namespace {
 thread_local int tl_err = OV_OK;
 thread_local char tl_msg[512] = "";
-thread_local OvStatsAcc tl_stats = {0, 0, 0, 0, 0, 0};
+thread_local OvStatsAcc tl_stats = {0, 0, 0, 0, 0, 0, 0};
 thread_local ov_state_impl* tl_last_state = nullptr;
 int g_precision = OV_PREC_FP64;
 int g_rk4_classic = 0;
@@ -474,7 +474,7 @@ bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* 
                    OvTree* external_tree) {
   (void)dxi;
   tl_last_state = s;
-  tl_stats = OvStatsAcc{0, 0, 0, 0, 0, 0};
+  tl_stats = OvStatsAcc{0, 0, 0, 0, 0, 0, 0};
   cudaEventRecord(s->ev0, s->stream);
   cudaEventRecord(s->ev1, s->stream);
   cudaEventRecord(s->ev2, s->stream);
@@ -510,6 +510,7 @@ bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* 
   s->acc_bs_launches += s->P.lia_only ? 0 : 1;
   s->acc_inter += tl_stats.interactions;
   s->acc_cells += tl_stats.cell_interactions;
+  s->acc_warp_iter += tl_stats.warp_iterations;
   return true;
 }
 
@@ -620,6 +621,7 @@ int ov_state_get_stats(ov_state* st, ov_run_stats* out) {
   out->launches = (double)(ov_launches() - s->launches_at_reset);
   out->n_targets = s->n_targets;
   out->n_segments = s->n_segments;
+  out->warp_iterations = s->acc_warp_iter;
   return OV_OK;
 }
 
@@ -627,6 +629,7 @@ void ov_state_reset_stats(ov_state* st) {
   if (!st) return;
   ov_state_impl* s = &st->impl;
   s->acc_evals = s->acc_inter = s->acc_cells = s->acc_bs_ms = s->acc_bs_launches = 0;
+  s->acc_warp_iter = 0;
   s->acc_build_ms = 0;
   s->launches_at_reset = ov_launches();
 }

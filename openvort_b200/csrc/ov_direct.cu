@@ -98,15 +98,19 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
   }
 }
 
-// Mixed form.  Source tile in FP32 offsets from the block origin O (the
-// block's first target's point for this image).
+// Mixed form.  Sources and targets are FP64 offsets from the block origin O
+// (the block's first target's point for this image) split into two FP32
+// parts, hi = fl32(p - O) and lo = fl32((p - O) - hi); R = (a_hi - t_hi) +
+// (a_lo - t_lo) then carries ~2 FP32 ulps of |R| itself, however far the
+// source and target are from O.
 __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int n_src,
                                                       const double* __restrict__ tpos,
                                                       const int2* __restrict__ tstatus,
                                                       const int* __restrict__ order, int n_t,
-                                                      double* __restrict__ part) {
-  __shared__ float4 sh_a[kTS];   // r1 - O, w = |ds|^2 * 16
-  __shared__ float4 sh_d[kTS];   // ds, w unused
+                                                      int stride, double* __restrict__ part) {
+  __shared__ float4 sh_hi[kTS];   // r1 - O (hi part), w = 16 |ds|^2
+  __shared__ float4 sh_lo[kTS];   // r1 - O (lo part)
+  __shared__ float4 sh_d[kTS];    // ds
   __shared__ int sh_id[kTS][2];
   __shared__ double sh_O[3];
   const int j = blockIdx.y;
@@ -127,7 +131,9 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int 
   __syncthreads();
   const d3 O = mk3(sh_O[0], sh_O[1], sh_O[2]);
   const int skip = (j == 0) ? k : -1;
-  const float tx = (float)(r.x - O.x), ty = (float)(r.y - O.y), tz = (float)(r.z - O.z);
+  const double ex = r.x - O.x, ey = r.y - O.y, ez = r.z - O.z;
+  const float thx = (float)ex, thy = (float)ey, thz = (float)ez;
+  const float tlx = (float)(ex - thx), tly = (float)(ey - thy), tlz = (float)(ez - thz);
   double ax = 0, ay = 0, az = 0;
   const float f4 = (float)P.f4pi;
   for (int base = 0; base < n_src; base += kTS) {
@@ -135,19 +141,22 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int 
     for (int q = threadIdx.x; q < kTS; q += kTB) {
       int m = base + q;
       int id = -1, fw = -1;
-      float4 a = make_float4(0, 0, 0, 0), d = make_float4(0, 0, 0, 0);
+      float4 hi = make_float4(0, 0, 0, 0), lo = make_float4(0, 0, 0, 0), d = make_float4(0, 0, 0, 0);
       if (m < n_src) {
         id = order ? order[m] : m;
         fw = S.fwd[id];
         if (fw >= 0) {
           const double* src = S.r1r2 + 6 * id;
           double dx = src[3] - src[0], dy = src[4] - src[1], dz = src[5] - src[2];
-          a = make_float4((float)(src[0] - O.x), (float)(src[1] - O.y), (float)(src[2] - O.z),
-                          (float)(16.0 * (dx * dx + dy * dy + dz * dz)));
+          double px = src[0] - O.x, py = src[1] - O.y, pz = src[2] - O.z;
+          float hx = (float)px, hy = (float)py, hz = (float)pz;
+          hi = make_float4(hx, hy, hz, (float)(16.0 * (dx * dx + dy * dy + dz * dz)));
+          lo = make_float4((float)(px - hx), (float)(py - hy), (float)(pz - hz), 0.f);
           d = make_float4((float)dx, (float)dy, (float)dz, 0.f);
         }
       }
-      sh_a[q] = a;
+      sh_hi[q] = hi;
+      sh_lo[q] = lo;
       sh_d[q] = d;
       sh_id[q][0] = id;
       sh_id[q][1] = fw;
@@ -160,9 +169,12 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int 
       float bx = 0, by = 0, bz = 0;
       int q1 = min(q0 + 32, cnt);
       for (int q = q0; q < q1; ++q) {
-        float4 a = sh_a[q];
-        float4 d = sh_d[q];
-        float Rx = a.x - tx, Ry = a.y - ty, Rz = a.z - tz;
+        const float4 a = sh_hi[q];
+        const float4 l = sh_lo[q];
+        const float4 d = sh_d[q];
+        float Rx = (a.x - thx) + (l.x - tlx);
+        float Ry = (a.y - thy) + (l.y - tly);
+        float Rz = (a.z - thz) + (l.z - tlz);
         float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
         if (R2 >= a.w && a.w > 0.f) {
           float vx, vy, vz;
@@ -180,7 +192,7 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int 
     }
   }
   if (k >= 0) {
-    double* o = part + (size_t)j * 3 * n_t + 3 * (size_t)k;
+    double* o = part + (size_t)j * 3 * stride + 3 * (size_t)k;
     o[0] = act ? ax : 0; o[1] = act ? ay : 0; o[2] = act ? az : 0;
   }
 }
@@ -236,7 +248,7 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
     if (!ov_tree_build(s, pos, &s->tree)) return false;
     k_direct_mixed<<<dim3((s->tree.n_nodes + kTB - 1) / kTB, nimg + 1), kTB, 0, s->stream>>>(
         s->P, S, s->tree.n_nodes, pos, s->status.as<int2>(), s->tree.perm.as<int>(), s->tree.n_nodes,
-        s->img_part.as<double>());
+        s->n, s->img_part.as<double>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
     // k_direct_mixed wrote part[j][k] for slots k in the sorted set only;

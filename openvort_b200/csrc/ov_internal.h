@@ -4,6 +4,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 #include <string>
 
@@ -30,37 +31,47 @@ struct DevBuf {
 
 // ---------------------------------------------------------------- BH tree
 // Octree cell kinds (what the walk does with a cell it reaches):
-//   CELL_LEAF     : N == 1, or the cell's box is below BH_grain: direct sum
-//                   over the cell's nodes, no opening test
+//   CELL_LEAF1    : a single node (N == 1): its segment, inline in the record
+//   CELL_LEAFN    : several nodes in a box below BH_grain: direct sum over the
+//                   cell's node range, no opening test
 //   CELL_OPEN     : opening test; on failure descend into the children
 //   CELL_OPEN_P2P : opening test; on failure direct sum over the cell's nodes
 //                   (a chain of single-child cells ending in a grain leaf)
-//   CELL_OPEN_ZERO: opening test; on failure nothing (unsplit or all nodes
+//   CELL_OPEN_ZERO: opening test; on failure nothing (unsplit, or every node
 //                   dropped from the children, src/octree.c:104,118-127)
-enum { CELL_LEAF = 0, CELL_OPEN = 1, CELL_OPEN_P2P = 2, CELL_OPEN_ZERO = 3 };
+enum { CELL_LEAF1 = 0, CELL_LEAFN = 1, CELL_OPEN = 2, CELL_OPEN_P2P = 3, CELL_OPEN_ZERO = 4 };
+#define CELL_KIND_SHIFT 29
+#define CELL_SKIP_MASK ((1 << CELL_KIND_SHIFT) - 1)
 
-// One cell in depth-first preorder.  Children of cell c start at c + 1;
-// the first cell after c's subtree is `skip`.
-struct __align__(16) CellMeta {
-  int start;   // first node (sorted order)
-  int count;   // nodes in the cell (including nodes dropped deeper down)
-  int skip;    // preorder index after this cell's subtree
-  int kind;    // CELL_*
-  double thr;  // opening test passes iff |r - com|^2 (reference wrapping) >= thr
-  double Lm;   // max box size at the tested level (for user-supplied theta)
+// One cell in depth-first preorder, one 128-byte line.  Children of cell c
+// start at c + 1; the first cell after c's subtree is `skip`.
+//   bytes   0-11  : a, b, skip | kind << 29
+//                   (LEAF1: a = node slot, b = forward slot;
+//                    otherwise a = first sorted node, b = node count)
+//   bytes  12-15  : FP32 m21
+//   bytes  16-23  : thr, the opening test passes iff the reference-wrapped
+//                   squared distance to the centre of mass is >= thr
+//   bytes  24-47  : x = centre of mass (LEAF1: segment start r1)
+//   bytes  48-71  : y = kappa/4pi * total circulation (LEAF1: wrapped r2)
+//   bytes  72-103 : kappa/4pi * (m21, m02, m12, m22), FP64
+//   bytes 104-127 : FP32 circulation and m02, m12, m22 (the mixed form reads
+//                   bytes 0-47 and 104-127 only)
+struct __align__(128) Cell {
+  int a, b, skip_kind;
+  float f_m21;
+  double thr;
+  double x[3];
+  double y[3];
+  double m[4];
+  float f_g[3];
+  float f_m02, f_m12, f_m22;
 };
-
-struct __align__(16) CellMom64 {  // kappa/4pi-scaled moments, FP64
-  double com[3];
-  double gam[3];                  // sum of segment vectors
-  double m21, m02, m12, m22;      // the circulation-tensor entries the expansion uses
-};
-
-struct __align__(16) CellMom32 {  // FP32 copy of the scaled moments
-  float gam[3];
-  float m21, m02, m12, m22;
-  float pad;
-};
+static_assert(sizeof(Cell) == 128, "cell record is one 128-byte line");
+// the walk loads these fields with vector loads of the given width
+static_assert(offsetof(Cell, a) % 16 == 0, "int4 header load");
+static_assert(offsetof(Cell, thr) % 16 == 0, "double2 (thr, x0) load");
+static_assert(offsetof(Cell, x) % 16 == 8 && (offsetof(Cell, x) + 8) % 16 == 0, "double2 (x1, x2) load");
+static_assert(offsetof(Cell, f_g) % 8 == 0 && offsetof(Cell, f_m12) % 8 == 0, "float2 loads");
 
 struct OvTree {
   int n_nodes = 0;      // active (non-EMPTY) nodes
@@ -72,7 +83,7 @@ struct OvTree {
   DevBuf perm;          // sorted index -> slot
   DevBuf bnode;         // binary radix tree nodes
   DevBuf cstart_cnt, cbase, cell_of;   // preorder bookkeeping
-  DevBuf meta, mom64, mom32;           // cells
+  DevBuf cells, cell_lm;               // cell records, max box side per cell
   DevBuf nodes64;       // per sorted node: r1 (3), r2 wrapped (3)
   DevBuf nodeids;       // per sorted node: slot, forward slot
   DevBuf nodes32;       // per sorted node: r1 - cell-free origin (FP32 not used yet)
@@ -101,6 +112,7 @@ struct ov_state_impl {
   double t_last = 0;
   // accumulated over evaluations since the last reset (ov_state_get_stats)
   double acc_evals = 0, acc_inter = 0, acc_cells = 0, acc_bs_ms = 0, acc_bs_launches = 0;
+  double acc_warp_iter = 0;
   double acc_build_ms = 0, last_run_ms = 0;
   long long launches_at_reset = 0;
   int n_targets = 0, n_segments = 0;
@@ -151,7 +163,7 @@ bool ov_state_reserve(ov_state_impl* s, int n);
 
 // per-thread statistics of the last evaluation
 struct OvStatsAcc {
-  double interactions, cell_interactions, cells, eval_ms, build_ms, total_ms;
+  double interactions, cell_interactions, cells, eval_ms, build_ms, total_ms, warp_iterations;
 };
 OvStatsAcc& ov_stats_tls();
 

@@ -343,7 +343,7 @@ __global__ void k_classify(const BNode* __restrict__ nodes, const int* __restric
   CellInfo ci;
   ci.ltop = ltop;
   ci.is_cell = ltop <= min(lbot, tl);
-  ci.kind = CELL_LEAF;
+  ci.kind = CELL_LEAF1;
   ci.mac_level = -1;
   if (ci.is_cell) {
     int N = last - first + 1;
@@ -351,10 +351,10 @@ __global__ void k_classify(const BNode* __restrict__ nodes, const int* __restric
     // the shared box; a drop at level tl+1 is shared only when tl+1 <= lbot
     bool ends = (tk == TERM_DROP) ? (tl < lbot) : (tl <= lbot);
     if (N == 1) {
-      ci.kind = CELL_LEAF;
+      ci.kind = CELL_LEAF1;
     } else if (ends) {
       if (tk == TERM_GRAIN) {
-        if (tl == ltop) ci.kind = CELL_LEAF;
+        if (tl == ltop) ci.kind = CELL_LEAFN;
         else { ci.kind = CELL_OPEN_P2P; ci.mac_level = tl - 1; }
       } else {  // unsplit (build stop) or every node dropped one level down
         ci.kind = CELL_OPEN_ZERO;
@@ -391,7 +391,8 @@ __device__ double mac_threshold(double Lm, double theta) {
 __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __restrict__ leaf_parent,
                               const CellInfo* __restrict__ info, const unsigned* __restrict__ base,
                               const uint64_t* __restrict__ khi, const uint64_t* __restrict__ klo,
-                              OvParams P, int n, CellMeta* meta, int* cell_level, int* lists,
+                              const double* __restrict__ nodes64, const int2* __restrict__ nodeids,
+                              OvParams P, int n, Cell* cells, double* cell_lm, int* lists,
                               int* list_counts) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= 2 * n - 1) return;
@@ -403,33 +404,44 @@ __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __rest
   for (int p = parent; p >= 0 && nodes[p].first == first; p = nodes[p].parent)
     if (info[p].is_cell) ++rank;
   int idx = base[first] + rank;
-  CellMeta m;
-  m.start = first;
-  m.count = last - first + 1;
-  m.skip = base[last + 1];
-  m.kind = ci.kind;
-  m.thr = DBL_MAX;
-  m.Lm = 0;
+  Cell c;
+  memset(&c, 0, sizeof(c));
+  int skip = (int)base[last + 1];
+  c.skip_kind = skip | (ci.kind << CELL_KIND_SHIFT);
+  c.thr = DBL_MAX;
+  double Lm = 0;
+  if (ci.kind == CELL_LEAF1) {
+    // the node's segment inline (segment_field, src/tangle.c:519-528)
+    const double* nd = nodes64 + 6 * (size_t)first;
+    int2 id = nodeids[first];
+    c.a = id.x;
+    c.b = id.y;
+    for (int q = 0; q < 3; ++q) { c.x[q] = nd[q]; c.y[q] = nd[3 + q]; }
+  } else {
+    c.a = first;
+    c.b = last - first + 1;
+  }
   if (ci.mac_level >= 0) {
     // replay the descent to the tested level to get the reference's box
     double lo[3] = {P.lo[0], P.lo[1], P.lo[2]}, hi[3] = {P.hi[0], P.hi[1], P.hi[2]};
     uint64_t h = khi[first], l = klo[first];
     for (int lev = 1; lev <= ci.mac_level; ++lev) {
-      double c[3], Lh[3], clo[3], chi[3];
-      split_params(lo, hi, c, Lh);
-      child_box(lo, hi, c, Lh, key_digit(h, l, lev), P.quadtree, clo, chi);
+      double cc[3], Lh[3], clo[3], chi[3];
+      split_params(lo, hi, cc, Lh);
+      child_box(lo, hi, cc, Lh, key_digit(h, l, lev), P.quadtree, clo, chi);
 #pragma unroll
       for (int a = 0; a < 3; ++a) { lo[a] = clo[a]; hi[a] = chi[a]; }
     }
-    m.Lm = box_max(lo, hi);
-    m.thr = mac_threshold(m.Lm, P.theta);
+    Lm = box_max(lo, hi);
+    c.thr = mac_threshold(Lm, P.theta);
     // moments are needed: file the cell by size for the moment kernels
-    int cls = m.count <= 16 ? 0 : (m.count <= 4096 ? 1 : 2);
+    int count = last - first + 1;
+    int cls = count <= 16 ? 0 : (count <= 4096 ? 1 : 2);
     int slot = atomicAdd(&list_counts[cls], 1);
     lists[cls * (size_t)(2 * n) + slot] = idx;
   }
-  meta[idx] = m;
-  cell_level[idx] = ci.mac_level;
+  cells[idx] = c;
+  cell_lm[idx] = Lm;
 }
 
 // ---------------------------------------------------------------- 5. nodes + moments
@@ -447,23 +459,19 @@ __global__ void k_nodes(OvParams P, const int* __restrict__ perm, const double* 
   nodeids[i] = make_int2(k, f);
 }
 
-struct MomAcc {
-  double sx, sy, sz;
-};
-
-__device__ __forceinline__ void write_moments(const CellMeta& m, d3 com, d3 g, double m21, double m02,
-                                              double m12, double m22, double f4pi, CellMom64* o64,
-                                              CellMom32* o32) {
-  CellMom64 a;
-  a.com[0] = com.x; a.com[1] = com.y; a.com[2] = com.z;
-  a.gam[0] = g.x * f4pi; a.gam[1] = g.y * f4pi; a.gam[2] = g.z * f4pi;
-  a.m21 = m21 * f4pi; a.m02 = m02 * f4pi; a.m12 = m12 * f4pi; a.m22 = m22 * f4pi;
-  *o64 = a;
-  CellMom32 b;
-  b.gam[0] = (float)a.gam[0]; b.gam[1] = (float)a.gam[1]; b.gam[2] = (float)a.gam[2];
-  b.m21 = (float)a.m21; b.m02 = (float)a.m02; b.m12 = (float)a.m12; b.m22 = (float)a.m22;
-  b.pad = 0.f;
-  *o32 = b;
+// Moments into the cell record: com, and kappa/4pi-scaled circulation and
+// the four tensor entries the expansion reads, in FP64 and FP32.
+__device__ __forceinline__ void write_moments(Cell* c, d3 com, d3 g, double m21, double m02,
+                                              double m12, double m22, double f4pi) {
+  double gs[3] = {g.x * f4pi, g.y * f4pi, g.z * f4pi};
+  double ms[4] = {m21 * f4pi, m02 * f4pi, m12 * f4pi, m22 * f4pi};
+  c->x[0] = com.x; c->x[1] = com.y; c->x[2] = com.z;
+  for (int q = 0; q < 3; ++q) { c->y[q] = gs[q]; c->f_g[q] = (float)gs[q]; }
+  for (int q = 0; q < 4; ++q) c->m[q] = ms[q];
+  c->f_m21 = (float)ms[0];
+  c->f_m02 = (float)ms[1];
+  c->f_m12 = (float)ms[2];
+  c->f_m22 = (float)ms[3];
 }
 
 // Moments over a node range, one thread per cell (octree_update_means,
@@ -471,23 +479,22 @@ __device__ __forceinline__ void write_moments(const CellMeta& m, d3 com, d3 g, d
 // segment vectors; M = sum ds (x) (r - com).  Only the four entries of M the
 // expansion reads are kept.
 __global__ void k_moments_thread(const int* __restrict__ list, const int* __restrict__ list_count,
-                                 const CellMeta* __restrict__ meta, const double* __restrict__ nodes64,
-                                 const int2* __restrict__ nodeids, double f4pi, CellMom64* mom64,
-                                 CellMom32* mom32) {
+                                 Cell* cells, const double* __restrict__ nodes64,
+                                 const int2* __restrict__ nodeids, double f4pi) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= *list_count) return;
   int c = list[t];
-  CellMeta m = meta[c];
+  const int start = cells[c].a, count = cells[c].b;
   double sx = 0, sy = 0, sz = 0;
-  for (int i = m.start; i < m.start + m.count; ++i) {
+  for (int i = start; i < start + count; ++i) {
     const double* p = nodes64 + 6 * (size_t)i;
     sx += p[0]; sy += p[1]; sz += p[2];
   }
-  double inv = 1.0 / m.count;
+  double inv = 1.0 / count;
   d3 com = mk3(sx * inv, sy * inv, sz * inv);
   d3 g = mk3(0, 0, 0);
   double m21 = 0, m02 = 0, m12 = 0, m22 = 0;
-  for (int i = m.start; i < m.start + m.count; ++i) {
+  for (int i = start; i < start + count; ++i) {
     if (nodeids[i].y < 0) continue;
     const double* p = nodes64 + 6 * (size_t)i;
     d3 ds = mk3(p[3] - p[0], p[4] - p[1], p[5] - p[2]);
@@ -495,22 +502,20 @@ __global__ void k_moments_thread(const int* __restrict__ list, const int* __rest
     g = g + ds;
     m21 += ds.z * loc.y; m02 += ds.x * loc.z; m12 += ds.y * loc.z; m22 += ds.z * loc.z;
   }
-  write_moments(m, com, g, m21, m02, m12, m22, f4pi, mom64 + c, mom32 + c);
+  write_moments(cells + c, com, g, m21, m02, m12, m22, f4pi);
 }
 
 // same, one warp per cell (17..4096 nodes) or one block per cell (larger)
 template <int kThreads>
-__device__ void moments_group(int c, const CellMeta* __restrict__ meta,
-                              const double* __restrict__ nodes64, const int2* __restrict__ nodeids,
-                              double f4pi, CellMom64* mom64, CellMom32* mom32, double* sh) {
+__device__ void moments_group(int c, Cell* cells, const double* __restrict__ nodes64,
+                              const int2* __restrict__ nodeids, double f4pi, double* sh) {
   const int tid = kThreads == 32 ? (threadIdx.x & 31) : threadIdx.x;
-  CellMeta m = meta[c];
+  const int start = cells[c].a, count = cells[c].b;
   double s[3] = {0, 0, 0};
-  for (int i = m.start + tid; i < m.start + m.count; i += kThreads) {
+  for (int i = start + tid; i < start + count; i += kThreads) {
     const double* p = nodes64 + 6 * (size_t)i;
     s[0] += p[0]; s[1] += p[1]; s[2] += p[2];
   }
-  // reduce
   for (int q = 0; q < 3; ++q) {
     double v = s[q];
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
@@ -531,10 +536,10 @@ __device__ void moments_group(int c, const CellMeta* __restrict__ meta,
     for (int q = 0; q < 3; ++q) s[q] = sh[256 + q];
     __syncthreads();
   }
-  double inv = 1.0 / m.count;
+  double inv = 1.0 / count;
   d3 com = mk3(s[0] * inv, s[1] * inv, s[2] * inv);
   double a[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int i = m.start + tid; i < m.start + m.count; i += kThreads) {
+  for (int i = start + tid; i < start + count; i += kThreads) {
     if (nodeids[i].y < 0) continue;
     const double* p = nodes64 + 6 * (size_t)i;
     double dx = p[3] - p[0], dy = p[4] - p[1], dz = p[5] - p[2];
@@ -559,33 +564,37 @@ __device__ void moments_group(int c, const CellMeta* __restrict__ meta,
       }
     }
   }
-  if (tid == 0)
-    write_moments(m, com, mk3(a[0], a[1], a[2]), a[3], a[4], a[5], a[6], f4pi, mom64 + c, mom32 + c);
+  if (tid == 0) write_moments(cells + c, com, mk3(a[0], a[1], a[2]), a[3], a[4], a[5], a[6], f4pi);
 }
 
 __global__ void k_moments_warp(const int* __restrict__ list, const int* __restrict__ list_count,
-                               const CellMeta* __restrict__ meta, const double* __restrict__ nodes64,
-                               const int2* __restrict__ nodeids, double f4pi, CellMom64* mom64,
-                               CellMom32* mom32) {
+                               Cell* cells, const double* __restrict__ nodes64,
+                               const int2* __restrict__ nodeids, double f4pi) {
   int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= *list_count) return;
-  moments_group<32>(list[w], meta, nodes64, nodeids, f4pi, mom64, mom32, nullptr);
+  moments_group<32>(list[w], cells, nodes64, nodeids, f4pi, nullptr);
 }
 
 __global__ void k_moments_block(const int* __restrict__ list, const int* __restrict__ list_count,
-                                const CellMeta* __restrict__ meta, const double* __restrict__ nodes64,
-                                const int2* __restrict__ nodeids, double f4pi, CellMom64* mom64,
-                                CellMom32* mom32) {
+                                Cell* cells, const double* __restrict__ nodes64,
+                                const int2* __restrict__ nodeids, double f4pi) {
   __shared__ double sh[264];
   if ((int)blockIdx.x >= *list_count) return;
-  moments_group<256>(list[blockIdx.x], meta, nodes64, nodeids, f4pi, mom64, mom32, sh);
+  moments_group<256>(list[blockIdx.x], cells, nodes64, nodeids, f4pi, sh);
 }
 
-__global__ void k_single_cell(CellMeta* meta, int* cell_level) {
-  CellMeta m;
-  m.start = 0; m.count = 1; m.skip = 1; m.kind = CELL_LEAF; m.thr = DBL_MAX; m.Lm = 0;
-  meta[0] = m;
-  cell_level[0] = -1;
+// a tangle of one node: the root is that node's leaf
+__global__ void k_single_cell(Cell* cells, double* cell_lm, const double* __restrict__ nodes64,
+                              const int2* __restrict__ nodeids) {
+  Cell c;
+  memset(&c, 0, sizeof(c));
+  c.a = nodeids[0].x;
+  c.b = nodeids[0].y;
+  c.skip_kind = 1 | (CELL_LEAF1 << CELL_KIND_SHIFT);
+  c.thr = DBL_MAX;
+  for (int q = 0; q < 3; ++q) { c.x[q] = nodes64[q]; c.y[q] = nodes64[3 + q]; }
+  cells[0] = c;
+  cell_lm[0] = 0;
 }
 
 }  // namespace
@@ -593,8 +602,8 @@ __global__ void k_single_cell(CellMeta* meta, int* cell_level) {
 // ---------------------------------------------------------------- host driver
 void ov_tree_release(OvTree* t) {
   DevBuf* bufs[] = {&t->keys, &t->keys_alt, &t->vals, &t->vals_alt, &t->stop, &t->hist,
-                    &t->perm, &t->bnode, &t->cstart_cnt, &t->cbase, &t->cell_of, &t->meta,
-                    &t->mom64, &t->mom32, &t->nodes64, &t->nodeids, &t->nodes32, &t->counters,
+                    &t->perm, &t->bnode, &t->cstart_cnt, &t->cbase, &t->cell_of, &t->cells,
+                    &t->cell_lm, &t->nodes64, &t->nodeids, &t->nodes32, &t->counters,
                     &t->scratch};
   for (DevBuf* b : bufs) b->release();
   t->n_nodes = t->n_cells = t->built = 0;
@@ -696,22 +705,21 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
   if (!T->bnode.reserve(bn_bytes) ||
       !T->cstart_cnt.reserve(sizeof(CellInfo) * (size_t)nbin) ||
       !T->cbase.reserve(sizeof(unsigned) * (size_t)(na + 1)) ||
-      !T->meta.reserve(sizeof(CellMeta) * (size_t)nbin) ||
-      !T->cell_of.reserve(sizeof(int) * ((size_t)nbin + 3 * 2 * (size_t)na) + 64) ||
-      !T->mom64.reserve(sizeof(CellMom64) * (size_t)nbin) ||
-      !T->mom32.reserve(sizeof(CellMom32) * (size_t)nbin))
+      !T->cells.reserve(sizeof(Cell) * (size_t)nbin) ||
+      !T->cell_lm.reserve(sizeof(double) * (size_t)nbin) ||
+      !T->cell_of.reserve(sizeof(int) * (3 * 2 * (size_t)na) + 64))
     return false;
   BNode* bn = T->bnode.as<BNode>();
   int* leaf_parent = reinterpret_cast<int*>(reinterpret_cast<char*>(T->bnode.p) +
                                             sizeof(BNode) * (size_t)(na > 1 ? na - 1 : 1));
   CellInfo* info = T->cstart_cnt.as<CellInfo>();
   unsigned* base = T->cbase.as<unsigned>();
-  int* cell_level = T->cell_of.as<int>();
-  int* lists = cell_level + nbin;
+  int* lists = T->cell_of.as<int>();
   int* list_counts = ctr + 4;
-  CellMeta* meta = T->meta.as<CellMeta>();
+  Cell* cells = T->cells.as<Cell>();
+  double* cell_lm = T->cell_lm.as<double>();
   if (na == 1) {
-    k_single_cell<<<1, 1, 0, st>>>(meta, cell_level);
+    k_single_cell<<<1, 1, 0, st>>>(cells, cell_lm, T->nodes64.as<double>(), T->nodeids.as<int2>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
     T->n_cells = 1;
@@ -724,7 +732,8 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     k_scan_excl<<<1, 1024, 0, st>>>(base, na + 1);
     OV_LAUNCHED();
     k_write_cells<<<(nbin + 255) / 256, 256, 0, st>>>(bn, leaf_parent, info, base, hi_sorted, klo,
-                                                      s->P, na, meta, cell_level, lists, list_counts);
+                                                      T->nodes64.as<double>(), T->nodeids.as<int2>(),
+                                                      s->P, na, cells, cell_lm, lists, list_counts);
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
     unsigned nc = 0;
@@ -735,21 +744,19 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     T->n_cells = (int)nc;
     const double f4 = s->P.f4pi;
     if (lc[0] > 0) {
-      k_moments_thread<<<(lc[0] + 127) / 128, 128, 0, st>>>(lists, list_counts, meta,
-                                                            T->nodes64.as<double>(), T->nodeids.as<int2>(),
-                                                            f4, T->mom64.as<CellMom64>(), T->mom32.as<CellMom32>());
+      k_moments_thread<<<(lc[0] + 127) / 128, 128, 0, st>>>(lists, list_counts, cells,
+                                                            T->nodes64.as<double>(), T->nodeids.as<int2>(), f4);
       OV_LAUNCHED();
     }
     if (lc[1] > 0) {
-      k_moments_warp<<<(lc[1] * 32 + 255) / 256, 256, 0, st>>>(lists + 2 * (size_t)na, list_counts + 1, meta,
-                                                              T->nodes64.as<double>(), T->nodeids.as<int2>(),
-                                                              f4, T->mom64.as<CellMom64>(), T->mom32.as<CellMom32>());
+      k_moments_warp<<<(lc[1] * 32 + 255) / 256, 256, 0, st>>>(lists + 2 * (size_t)na, list_counts + 1,
+                                                              cells, T->nodes64.as<double>(),
+                                                              T->nodeids.as<int2>(), f4);
       OV_LAUNCHED();
     }
     if (lc[2] > 0) {
-      k_moments_block<<<lc[2], 256, 0, st>>>(lists + 4 * (size_t)na, list_counts + 2, meta,
-                                             T->nodes64.as<double>(), T->nodeids.as<int2>(), f4,
-                                             T->mom64.as<CellMom64>(), T->mom32.as<CellMom32>());
+      k_moments_block<<<lc[2], 256, 0, st>>>(lists + 4 * (size_t)na, list_counts + 2, cells,
+                                             T->nodes64.as<double>(), T->nodeids.as<int2>(), f4);
       OV_LAUNCHED();
     }
     OV_TRY_CUDA(cudaGetLastError());

@@ -26,9 +26,8 @@
 namespace {
 
 struct TreeView {
-  const CellMeta* meta;
-  const CellMom64* mom64;
-  const CellMom32* mom32;
+  const Cell* cells;
+  const double* cell_lm;   // max box side per cell (opening test at a user theta)
   const double* nodes64;   // per sorted node: r1, wrapped r2
   const int2* nodeids;     // per sorted node: slot, forward slot
   int n_cells;
@@ -38,12 +37,13 @@ struct TreeView {
 // squared distance from r to the cell's centre of mass after the reference's
 // one-box wrap of the centre (seg_pwrap + segment_len, src/octree.c:286-287),
 // with exactly its FP64 operations
-__device__ __forceinline__ double mac_dist2(const OvParams& P, d3 r, const double* com) {
+__device__ __forceinline__ double mac_dist2(const OvParams& P, d3 r, double cx, double cy, double cz) {
   double u[3];
   const double rr[3] = {r.x, r.y, r.z};
+  const double cc[3] = {cx, cy, cz};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double c = com[a];
+    double c = cc[a];
     if (P.periodic[a]) {
       double d = __dsub_rn(c, rr[a]);
       if (d > P.L[a] * 0.5) c = __dsub_rn(c, P.L[a]);
@@ -60,109 +60,137 @@ __device__ __forceinline__ double mac_dist2(const OvParams& P, d3 r, const doubl
 // The reference's expansion (src/octree.c:303-328), moments pre-scaled by
 // kappa/4pi: gam x R / |R|^3 + (M21, 0, 0) / |R|^3 + (M.2 R_z) x R / |R|^5,
 // where (M.2 R_z) = (M02 Rz, M12 Rz, M22 Rz) is what its mat3_vmul returns.
-__device__ __forceinline__ d3 expansion64(const CellMom64& m, d3 R) {
+__device__ __forceinline__ d3 expansion64(const double* g, const double* m, d3 R) {
   double R2 = dot3(R, R);
   double inv = 1.0 / sqrt(R2);
   double i3 = inv * inv * inv;
   double i5 = i3 * inv * inv;
-  d3 g = mk3(m.gam[0], m.gam[1], m.gam[2]);
-  d3 v = cross3(g, R) * i3;
-  v.x += m.m21 * i3;
-  d3 mv = mk3(m.m02 * R.z, m.m12 * R.z, m.m22 * R.z);
+  d3 v = cross3(mk3(g[0], g[1], g[2]), R) * i3;
+  v.x += m[0] * i3;
+  d3 mv = mk3(m[1] * R.z, m[2] * R.z, m[3] * R.z);
   return v + cross3(mv, R) * i5;
 }
 
-__device__ __forceinline__ void expansion32(const CellMom32& m, float Rx, float Ry, float Rz,
+__device__ __forceinline__ void expansion32(float g0, float g1, float g2, float m21, float m02,
+                                            float m12, float m22, float Rx, float Ry, float Rz,
                                             float& vx, float& vy, float& vz) {
   float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
   float inv = rsqrtf(R2);
   float i3 = inv * inv * inv;
   float i5 = i3 * inv * inv;
-  float cx = m.gam[1] * Rz - m.gam[2] * Ry;
-  float cy = m.gam[2] * Rx - m.gam[0] * Rz;
-  float cz = m.gam[0] * Ry - m.gam[1] * Rx;
-  float ax = m.m02 * Rz, ay = m.m12 * Rz, az = m.m22 * Rz;
+  float cx = g1 * Rz - g2 * Ry;
+  float cy = g2 * Rx - g0 * Rz;
+  float cz = g0 * Ry - g1 * Rx;
+  float ax = m02 * Rz, ay = m12 * Rz, az = m22 * Rz;
   float qx = ay * Rz - az * Ry, qy = az * Rx - ax * Rz, qz = ax * Ry - ay * Rx;
-  vx = fmaf(cx + m.m21, i3, qx * i5);
+  vx = fmaf(cx + m21, i3, qx * i5);
   vy = fmaf(cy, i3, qy * i5);
   vz = fmaf(cz, i3, qz * i5);
 }
 
-enum { ACT_NONE = 0, ACT_P2P = 1, ACT_FAR = 2, ACT_OPEN = 3 };
+__device__ __forceinline__ void prefetch_l1(const void* p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
 
-// One walk of one warp: lane targets rp (valid if `live`), skip rule `skip`.
-// Returns the lane's sum; counts interactions.
+enum { ACT_NONE = 0, ACT_P2P1 = 1, ACT_P2PN = 2, ACT_FAR = 3, ACT_OPEN = 4 };
+
+// One segment at rp: FP64 with the reference's cut-offs, or (mixed, far
+// segments |R| >= 4 |ds|) FP32 from FP64-formed R and ds.
+template <bool kMixed>
+__device__ __forceinline__ void p2p_one(const OvParams& P, d3 r1, d3 r2, d3 rp, double& ax,
+                                        double& ay, double& az) {
+  if (kMixed) {
+    d3 R = r1 - rp;
+    d3 ds = r2 - r1;
+    double R2 = dot3(R, R), ds2 = dot3(ds, ds);
+    if (R2 >= 16.0 * ds2 && ds2 > 0) {
+      float vx, vy, vz;
+      seg_vel32((float)P.f4pi, (float)R.x, (float)R.y, (float)R.z, (float)ds.x, (float)ds.y,
+                (float)ds.z, vx, vy, vz);
+      ax += vx; ay += vy; az += vz;
+      return;
+    }
+  }
+  d3 v = seg_vel64(P.f4pi, r1, r2, rp);
+  ax += v.x; ay += v.y; az += v.z;
+}
+
+// One walk of one warp: lane target rp (valid if `live`), skip rule `skip`.
+// Each visited cell is one 128-byte record, loaded once for the warp; both
+// possible successors (first child q+1 and skip) are prefetched into L1.
 template <bool kMixed>
 __device__ d3 warp_walk(const OvParams& P, const TreeView& T, d3 rp, bool live, int skip,
                         bool use_thr, double theta, unsigned long long& n_p2p,
-                        unsigned long long& n_far) {
+                        unsigned long long& n_far, unsigned long long& n_iter) {
   const unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
   int next = live ? 0 : T.n_cells;
   double ax = 0, ay = 0, az = 0;
   for (;;) {
-    int q = __reduce_min_sync(FULL, (unsigned)next);
+    const int q = (int)__reduce_min_sync(FULL, (unsigned)next);
     if (q >= T.n_cells) break;
-    const CellMeta m = T.meta[q];
+    const Cell* cp = T.cells + q;
+    if (lane == 0 && q + 1 < T.n_cells) prefetch_l1(cp + 1);
+    const int4 h = *reinterpret_cast<const int4*>(cp);           // a, b, skip|kind, f_m21
+    const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);  // thr, x0
+    const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]); // x1, x2
+    const int kind = (unsigned)h.z >> CELL_KIND_SHIFT;
+    const int skp = h.z & CELL_SKIP_MASK;
+    if (lane == 1 && skp < T.n_cells) prefetch_l1(T.cells + skp);
     int act = ACT_NONE;
     if (next == q) {
-      if (m.kind == CELL_LEAF) {
-        act = ACT_P2P;
+      if (kind == CELL_LEAF1) {
+        act = ACT_P2P1;
+      } else if (kind == CELL_LEAFN) {
+        act = ACT_P2PN;
       } else {
-        const double* com = T.mom64[q].com;
-        double s = mac_dist2(P, rp, com);
-        bool pass = use_thr ? (s >= m.thr)
-                            : (s > 0 && __ddiv_rn(m.Lm, __dsqrt_rn(s)) < theta);
+        double s = mac_dist2(P, rp, t0.y, t1.x, t1.y);
+        bool pass = use_thr ? (s >= t0.x)
+                            : (s > 0 && __ddiv_rn(T.cell_lm[q], __dsqrt_rn(s)) < theta);
         if (pass) act = ACT_FAR;
-        else if (m.kind == CELL_OPEN) act = ACT_OPEN;
-        else if (m.kind == CELL_OPEN_P2P) act = ACT_P2P;
-        else act = ACT_NONE;
+        else if (kind == CELL_OPEN) act = ACT_OPEN;
+        else if (kind == CELL_OPEN_P2P) act = ACT_P2PN;
       }
       // every lane's next cell strictly increases, so a walk ends within
       // n_cells iterations whatever the cell records hold
-      next = (act == ACT_OPEN) ? q + 1 : max(m.skip, q + 1);
+      next = (act == ACT_OPEN) ? q + 1 : max(skp, q + 1);
     }
     if (act == ACT_FAR) {
       if (kMixed) {
-        const double* com = T.mom64[q].com;
-        float Rx = (float)(rp.x - com[0]), Ry = (float)(rp.y - com[1]), Rz = (float)(rp.z - com[2]);
+        // bytes 104-127 are 8-byte aligned: three float2 loads
+        const float2 f0 = *reinterpret_cast<const float2*>(&cp->f_g[0]);  // g0 g1
+        const float2 f1 = *reinterpret_cast<const float2*>(&cp->f_g[2]);  // g2 m02
+        const float2 f2 = *reinterpret_cast<const float2*>(&cp->f_m12);   // m12 m22
         float vx, vy, vz;
-        expansion32(T.mom32[q], Rx, Ry, Rz, vx, vy, vz);
+        expansion32(f0.x, f0.y, f1.x, __int_as_float(h.w), f1.y, f2.x, f2.y, (float)(rp.x - t0.y),
+                    (float)(rp.y - t1.x), (float)(rp.z - t1.y), vx, vy, vz);
         ax += vx; ay += vy; az += vz;
       } else {
-        const CellMom64 mm = T.mom64[q];
-        d3 R = mk3(rp.x - mm.com[0], rp.y - mm.com[1], rp.z - mm.com[2]);
-        d3 v = expansion64(mm, R);
+        d3 v = expansion64(cp->y, cp->m, mk3(rp.x - t0.y, rp.y - t1.x, rp.z - t1.y));
         ax += v.x; ay += v.y; az += v.z;
       }
+    } else if (act == ACT_P2P1) {
+      // skip rule of calculate_vs_shift (src/tangle.c:567-569)
+      if (h.y != -1 && h.x != skip && h.y != skip)
+        p2p_one<kMixed>(P, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), rp, ax, ay, az);
     }
-    unsigned far_mask = __ballot_sync(FULL, act == ACT_FAR);
-    unsigned p2p_mask = __ballot_sync(FULL, act == ACT_P2P);
-    if (lane == 0) n_far += __popc(far_mask);
-    if (p2p_mask) {
-      const int end = min(m.start + m.count, T.n_nodes);
-      if (lane == 0) n_p2p += (unsigned long long)__popc(p2p_mask) * m.count;
-      for (int i = max(m.start, 0); i < end; ++i) {
+    const unsigned far_mask = __ballot_sync(FULL, act == ACT_FAR);
+    const unsigned p1_mask = __ballot_sync(FULL, act == ACT_P2P1);
+    const unsigned pn_mask = __ballot_sync(FULL, act == ACT_P2PN);
+    if (lane == 0) {
+      n_far += __popc(far_mask);
+      n_p2p += __popc(p1_mask);
+      ++n_iter;
+    }
+    if (pn_mask) {
+      const int end = min(h.x + h.y, T.n_nodes);
+      if (lane == 0) n_p2p += (unsigned long long)__popc(pn_mask) * h.y;
+      for (int i = max(h.x, 0); i < end; ++i) {
         const int2 id = T.nodeids[i];
-        if (act != ACT_P2P) continue;
-        // skip rule of calculate_vs_shift (src/tangle.c:567-569)
+        if (act != ACT_P2PN) continue;
         if (id.y == -1 || id.x == skip || id.y == skip) continue;
         const double* nd = T.nodes64 + 6 * (size_t)i;
-        d3 r1 = mk3(nd[0], nd[1], nd[2]), r2 = mk3(nd[3], nd[4], nd[5]);
-        if (kMixed) {
-          d3 R = r1 - rp;
-          d3 ds = r2 - r1;
-          double R2 = dot3(R, R), ds2 = dot3(ds, ds);
-          if (R2 >= 16.0 * ds2 && ds2 > 0) {
-            float vx, vy, vz;
-            seg_vel32((float)P.f4pi, (float)R.x, (float)R.y, (float)R.z, (float)ds.x, (float)ds.y,
-                      (float)ds.z, vx, vy, vz);
-            ax += vx; ay += vy; az += vz;
-            continue;
-          }
-        }
-        d3 v = seg_vel64(P.f4pi, r1, r2, rp);
-        ax += v.x; ay += v.y; az += v.z;
+        p2p_one<kMixed>(P, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), rp, ax, ay, az);
       }
     }
   }
@@ -185,12 +213,12 @@ __global__ void __launch_bounds__(128) k_walk_nodes(OvParams P, TreeView T, cons
   int k = i < n_t ? (order ? order[i] : i) : -1;
   bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
   d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
-  unsigned long long n_p2p = 0, n_far = 0;
-  d3 nl = warp_walk<kMixed>(P, T, r, live, k, true, P.theta, n_p2p, n_far);
+  unsigned long long n_p2p = 0, n_far = 0, n_iter = 0;
+  d3 nl = warp_walk<kMixed>(P, T, r, live, k, true, P.theta, n_p2p, n_far, n_iter);
   d3 im = mk3(0, 0, 0);
   for (int j = 0; j < P.n_img; ++j) {
     d3 rp = live ? image_point(P, j, r) : r;
-    d3 v = warp_walk<kMixed>(P, T, rp, live, -1, true, P.theta, n_p2p, n_far);
+    d3 v = warp_walk<kMixed>(P, T, rp, live, -1, true, P.theta, n_p2p, n_far, n_iter);
     int face = P.img[j][3];
     if (face > -1) v = mirror_dir(v, face);
     im = im + v;
@@ -202,6 +230,7 @@ __global__ void __launch_bounds__(128) k_walk_nodes(OvParams P, TreeView T, cons
   if (lane == 0) {
     atomicAdd(&counters[0], n_p2p);
     atomicAdd(&counters[1], n_far);
+    atomicAdd(&counters[2], n_iter);
   }
 }
 
@@ -218,13 +247,13 @@ __global__ void __launch_bounds__(128) k_walk_points(OvParams P, TreeView T, con
   bool live = i < npts;
   d3 r = live ? ld3(pts, i) : mk3(0, 0, 0);
   int sk = (live && skip) ? skip[i] : -1;
-  unsigned long long n_p2p = 0, n_far = 0;
-  d3 v = warp_walk<kMixed>(P, T, r, live, sk, use_thr != 0, theta, n_p2p, n_far);
+  unsigned long long n_p2p = 0, n_far = 0, n_iter = 0;
+  d3 v = warp_walk<kMixed>(P, T, r, live, sk, use_thr != 0, theta, n_p2p, n_far, n_iter);
   if (out_img) {
     d3 im = mk3(0, 0, 0);
     for (int j = 0; j < P.n_img; ++j) {
       d3 rp = live ? image_point(P, j, r) : r;
-      d3 w = warp_walk<kMixed>(P, T, rp, live, -1, use_thr != 0, theta, n_p2p, n_far);
+      d3 w = warp_walk<kMixed>(P, T, rp, live, -1, use_thr != 0, theta, n_p2p, n_far, n_iter);
       int face = P.img[j][3];
       if (face > -1) w = mirror_dir(w, face);
       im = im + w;
@@ -235,14 +264,14 @@ __global__ void __launch_bounds__(128) k_walk_points(OvParams P, TreeView T, con
   if (lane == 0) {
     atomicAdd(&counters[0], n_p2p);
     atomicAdd(&counters[1], n_far);
+    atomicAdd(&counters[2], n_iter);
   }
 }
 
 TreeView view_of(OvTree* t) {
   TreeView v;
-  v.meta = t->meta.as<CellMeta>();
-  v.mom64 = t->mom64.as<CellMom64>();
-  v.mom32 = t->mom32.as<CellMom32>();
+  v.cells = t->cells.as<Cell>();
+  v.cell_lm = t->cell_lm.as<double>();
   v.nodes64 = t->nodes64.as<double>();
   v.nodeids = t->nodeids.as<int2>();
   v.n_cells = t->n_cells;
@@ -253,20 +282,21 @@ TreeView view_of(OvTree* t) {
 }  // namespace
 
 static bool read_counters(ov_state_impl* s, OvTree* t) {
-  unsigned long long c[2] = {0, 0};
+  unsigned long long c[3] = {0, 0, 0};
   OV_TRY_CUDA(cudaMemcpyAsync(c, t->counters.as<char>() + 64, sizeof(c), cudaMemcpyDeviceToHost,
                               s->stream));
   OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
   OvStatsAcc& st = ov_stats_tls();
   st.interactions = (double)c[0];
   st.cell_interactions = (double)c[1];
+  st.warp_iterations = (double)c[2];
   return true;
 }
 
 bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own_tree,
                         double* v_nl, double* v_img) {
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(t->counters.as<char>() + 64);
-  OV_TRY_CUDA(cudaMemsetAsync(ctr, 0, 16, s->stream));
+  OV_TRY_CUDA(cudaMemsetAsync(ctr, 0, 24, s->stream));
   // a tree built from these positions: its key order; otherwise slot order
   const int* order = own_tree ? t->perm.as<int>() : nullptr;
   int n_t = own_tree ? t->n_nodes : s->n;
@@ -308,7 +338,7 @@ bool ov_tree_walk_points(ov_state_impl* s, OvTree* t, int npts, const double* pt
     return true;
   }
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(t->counters.as<char>() + 64);
-  OV_TRY_CUDA(cudaMemsetAsync(ctr, 0, 16, s->stream));
+  OV_TRY_CUDA(cudaMemsetAsync(ctr, 0, 24, s->stream));
   int warps = (npts + 31) / 32;
   int blocks = (warps * 32 + 127) / 128;
   TreeView tv = view_of(t);

@@ -298,12 +298,14 @@ class Params:
             ctype.in_dll(lib, sym).value = getattr(self, attr)
 
     def apply_flows(self, lib: C.CDLL):
-        """Write vn_conf / vs_conf / vb_conf by name (fun left NULL)."""
-        self._keep = []
+        """Write vn_conf / vs_conf / vb_conf by name (fun left NULL).  The
+        name strings stay referenced from the library handle."""
+        keepall = []
         for sym, flow in (("vn_conf", self.vn), ("vs_conf", self.vs), ("vb_conf", self.vb)):
             conf, keep = flow.vconf()
-            self._keep.append((conf, keep))
+            keepall.append((conf, keep))
             C.memmove(C.addressof(VConf.in_dll(lib, sym)), C.addressof(conf), C.sizeof(VConf))
+        lib._ov_flow_strings = keepall
 
 
 def perpendicular(d: Sequence[float]) -> np.ndarray:

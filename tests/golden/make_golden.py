@@ -12,6 +12,7 @@ as the reference's main loop does, src/main.c:112-114).
 """
 from __future__ import annotations
 
+import dataclasses
 import json
 import sys
 from dataclasses import asdict
@@ -43,7 +44,7 @@ def cases():
     t = G.random_ring_tangle(1, 20, 0.1, boundary="periodic-26")
     yield "periodic26_direct", t, per_p, {"rk4_steps": 2, "dt": 1e-6}
     for th in (0.3, 0.4, 0.5):
-        p = Params(**{**per_p.__dict__, "use_bh": 1, "bh_theta": th})
+        p = dataclasses.replace(per_p, use_bh=1, bh_theta=th)
         yield f"periodic26_bh{int(th * 10)}", t, p, {"rk4_steps": 1 if th == 0.4 else 0, "dt": 1e-6}
     # open boundaries, EMPTY holes between the nodes, hyperfriction on
     t2 = G.random_ring_tangle(2, 8, 0.1, boundary="open", empty_slots=17)
@@ -53,7 +54,7 @@ def cases():
                 max_curv_scale=0.2, vn=Flow("simple", {"external_v": (0.0, 0.3, 0.0)}),
                 vs=Flow("simple", {"external_v": (0.01, 0.0, 0.0)}))
     yield "open_empty_direct", t2, p2, {"rk4_steps": 1, "dt": 1e-6}
-    yield "open_empty_bh4", t2, Params(**{**p2.__dict__, "use_bh": 1, "bh_theta": 0.4}), {"rk4_steps": 0, "dt": 0}
+    yield "open_empty_bh4", t2, dataclasses.replace(p2, use_bh=1, bh_theta=0.4), {"rk4_steps": 0, "dt": 0}
     # a half ring pinned on a mirror wall: pinned stencils, mirror image, v_b
     w = G.wall_half_ring(64)
     pw = Params(core_a=1.3e-8, dl_max=2e-3, hyperfriction=0, alpha=0.05, alpha_p=0.01,

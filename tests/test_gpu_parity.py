@@ -9,6 +9,7 @@ Tolerances (max over nodes of |dv| / |v_ref|):
   mixed path  1e-5 on velocities
 """
 import ctypes as C
+import dataclasses
 
 import numpy as np
 import pytest
@@ -149,7 +150,7 @@ def test_point_queries(ov, oracle):
         lib.octree_get_vs(tree, C.byref(Vec3d((C.c_double * 3)(*pts[i]))), p.bh_theta, C.byref(res), skip[i])
         ov.check(lib)
         assert rel_err(np.array(res.p)[None], want[i:i + 1]) < TOL_V64
-    p2 = Params(**{**p.__dict__, "bh_theta": 0.25})
+    p2 = dataclasses.replace(p, bh_theta=0.25)
     want2 = oracle.bh_at(t, p2, pts[:2])
     for i in range(2):
         res = Vec3d()
@@ -195,21 +196,23 @@ def test_update_velocities_with_user_tree(ov):
 
 
 def test_eval_points_direct_and_bh(ov, oracle):
+    """ov_state_eval_points: direct and Barnes-Hut sums with the 26 images at
+    arbitrary points, against the oracle summing the tangle and each image
+    point the same way (src/tangle.c:611-638)."""
     t, p, _, _ = load("periodic26_bh5")
     ov.configure(p, 0)
     st = ov.DeviceState(t.copy())
     rng = np.random.default_rng(9)
     pts = rng.uniform(0, 0.1, size=(100, 3))
-    d = st.eval_points(pts, method=0)
-    # direct with images at points = the tangle's own sum + image sum
-    ref = oracle.segments_at(t, p, pts)
-    L = 0.1
     from openvort_b200.tangle import IMAGE_TABLES
+    L = 0.1
+    ref_d = oracle.segments_at(t, p, pts)
+    ref_b = oracle.bh_at(t, p, pts)
     for sh, _ in IMAGE_TABLES["periodic-26"]:
-        ref = ref + oracle.segments_at(t, p, pts - L * np.array(sh))
-    assert rel_err(d, ref) < TOL_V64
-    b = st.eval_points(pts, method=1)
-    assert 1e-6 < rel_err(b, ref) < 0.5
+        ref_d = ref_d + oracle.segments_at(t, p, pts - L * np.array(sh))
+        ref_b = ref_b + oracle.bh_at(t, p, pts - L * np.array(sh))
+    assert rel_err(st.eval_points(pts, method=0), ref_d) < TOL_V64
+    assert rel_err(st.eval_points(pts, method=1), ref_b) < TOL_V64
     st.close()
 
 
@@ -249,7 +252,7 @@ def test_unknown_flow_fails_loudly(ov, monkeypatch):
     t = G.single_ring(32, 1e-2)
     p = Params(use_mf=1, hyperfriction=0, vn=Flow("simple", {"external_v": (1, 0, 0)}))
     lib = ov.configure(p, 0)
-    conf, keep = Flow("simple").vconf()
+    conf, keep = Flow("simple", {"external_v": (1, 0, 0)}).vconf()
     conf.name = b"no such flow"
     C.memmove(C.addressof(type(conf).in_dll(lib, "vn_conf")), C.addressof(conf), C.sizeof(conf))
     with pytest.raises(ov.OVError) as e:
