@@ -229,6 +229,10 @@ int ov_get_precision(void);
  * (src/vortex_dynamics.c:89); 1: classic RK4 (fourth stage advances dt) */
 void ov_set_rk4_classic(int classic);
 int ov_get_rk4_classic(void);
+/* Mixed form: interactions closer than factor * global_dl_max to the target
+ * (segments and cell expansions) are evaluated in FP64 (default 16). */
+void ov_set_mixed_near_factor(double factor);
+double ov_get_mixed_near_factor(void);
 
 /* Per-call counters of the last velocity evaluation on this thread. */
 typedef struct {

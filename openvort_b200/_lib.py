@@ -29,6 +29,7 @@ FUNCTIONS = [
     "ov_state_create", "ov_state_destroy", "ov_state_upload", "ov_state_download",
     "ov_state_update_tangle", "ov_state_rk4_step", "ov_state_run", "ov_state_eval_points",
     "ov_measure_fma_peak", "ov_state_get_stats", "ov_state_reset_stats",
+    "ov_set_mixed_near_factor", "ov_get_mixed_near_factor",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -108,6 +109,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "shifted": (Vec3d, [C.c_void_p, T, V]),
         "ov_state_get_stats": (C.c_int, [C.c_void_p, C.POINTER(RunStats)]),
         "ov_state_reset_stats": (None, [C.c_void_p]),
+        "ov_set_mixed_near_factor": (None, [C.c_double]),
+        "ov_get_mixed_near_factor": (C.c_double, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -127,6 +127,7 @@ thread_local OvStatsAcc tl_stats = {0, 0, 0, 0, 0, 0, 0};
 thread_local ov_state_impl* tl_last_state = nullptr;
 int g_precision = OV_PREC_FP64;
 int g_rk4_classic = 0;
+double g_near_factor = 16.0;
 int g_device = -1;
 std::mutex g_init_mutex;
 }  // namespace
@@ -203,6 +204,8 @@ const char* ov_error_string(int code) {
 void ov_set_precision(int mode) { g_precision = mode == OV_PREC_MIXED ? OV_PREC_MIXED : OV_PREC_FP64; }
 int ov_get_precision(void) { return g_precision; }
 void ov_set_rk4_classic(int classic) { g_rk4_classic = classic ? 1 : 0; }
+void ov_set_mixed_near_factor(double f) { g_near_factor = f > 0 ? f : 0; }
+double ov_get_mixed_near_factor(void) { return g_near_factor; }
 int ov_get_rk4_classic(void) { return g_rk4_classic; }
 
 int ov_init(int device) {
@@ -349,6 +352,7 @@ bool capture_params(const tangle_state* t, OvParams& P, bool need_flows) {
   P.theta = global_BH_resolution;
   P.grain = global_BH_grain;
   P.dl_max = global_dl_max;
+  P.near2 = (g_near_factor * global_dl_max) * (g_near_factor * global_dl_max);
   P.alpha = global_alpha;
   P.alpha_p = global_alpha_p;
   P.max_curv = global_max_curvature_scale;

@@ -42,6 +42,7 @@ struct OvParams {
   int img[OV_MAX_IMAGES][4];    // shift x,y,z, reflect face (-1 none)
   int lia_only, use_bh, quadtree, use_mf, hyperfriction, precision;
   double theta, grain, dl_max;
+  double near2;                 // mixed form: squared radius of the FP64 near field
   double alpha, alpha_p, max_curv, hyperalpha;
   OvFlow vn, vs, vb;
 };
@@ -150,8 +151,13 @@ __device__ __forceinline__ d3 seg_vel64(double f4pi, d3 r1, d3 r2, d3 r) {
 // FP32 far-field form: R and the segment vector ds are formed in FP64 by the
 // caller and rounded once; R x R' = R x ds avoids the cancellation of the
 // product of two nearly parallel long vectors.  Only used where |R| >= 4|ds|,
-// where the reference's cut-offs cannot trigger.
-__device__ __forceinline__ void seg_vel32(float f4pi, float Rx, float Ry, float Rz,
+// where the reference's distance cut-off cannot trigger.  Its colinearity
+// cut-off |cos - 1| < 1e-8 (src/tangle.c:505-506) zeroes far segments that
+// point within ~1e-4 rad of the target, so it is applied here too, through
+// 1 - cos = |R x ds|^2 / (|R||R'| (|R||R'| + R.R')), which has no
+// cancellation.  Returns false when the test is within 2e-5 (relative) of
+// the threshold: the caller then evaluates the segment in FP64.
+__device__ __forceinline__ bool seg_vel32(float f4pi, float Rx, float Ry, float Rz,
                                           float dx, float dy, float dz,
                                           float& vx, float& vy, float& vz) {
   float Qx = Rx + dx, Qy = Ry + dy, Qz = Rz + dz;
@@ -161,10 +167,16 @@ __device__ __forceinline__ void seg_vel32(float f4pi, float Rx, float Ry, float 
   float ia = rsqrtf(R2), ib = rsqrtf(Q2);
   float a = R2 * ia, b = Q2 * ib;
   float ab = a * b;
+  float cx = Ry * dz - Rz * dy, cy = Rz * dx - Rx * dz, cz = Rx * dy - Ry * dx;
+  float C2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+  float den = ab * (ab + RQ);
+  vx = vy = vz = 0.f;
+  if (C2 < (1e-8f * (1.0f - 2e-5f)) * den) return true;   // colinear: zero
+  if (C2 <= (1e-8f * (1.0f + 2e-5f)) * den) return false; // too close to call
   // f (a+b) / (ab (ab + R.R'))
   float s = f4pi * (a + b) * ia * ib * __frcp_rn(ab + RQ);
-  float cx = Ry * dz - Rz * dy, cy = Rz * dx - Rx * dz, cz = Rx * dy - Ry * dx;
   vx = cx * s; vy = cy * s; vz = cz * s;
+  return true;
 }
 
 // ----------------------------------------------------------------------

@@ -98,7 +98,8 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
   }
 }
 
-// Mixed form.  Sources and targets are FP64 offsets from the block origin O
+// Mixed form.  Segments closer than max(4 |ds|, the near radius) use the
+// FP64 formula from the FP64 table.  Sources and targets are FP64 offsets from the block origin O
 // (the block's first target's point for this image) split into two FP32
 // parts, hi = fl32(p - O) and lo = fl32((p - O) - hi); R = (a_hi - t_hi) +
 // (a_lo - t_lo) then carries ~2 FP32 ulps of |R| itself, however far the
@@ -150,7 +151,8 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int 
           double dx = src[3] - src[0], dy = src[4] - src[1], dz = src[5] - src[2];
           double px = src[0] - O.x, py = src[1] - O.y, pz = src[2] - O.z;
           float hx = (float)px, hy = (float)py, hz = (float)pz;
-          hi = make_float4(hx, hy, hz, (float)(16.0 * (dx * dx + dy * dy + dz * dz)));
+          // FP32 beyond max(4 |ds|, the near radius)
+          hi = make_float4(hx, hy, hz, (float)fmax(16.0 * (dx * dx + dy * dy + dz * dz), P.near2));
           lo = make_float4((float)(px - hx), (float)(py - hy), (float)(pz - hz), 0.f);
           d = make_float4((float)dx, (float)dy, (float)dz, 0.f);
         }
@@ -176,13 +178,14 @@ __global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int 
         float Ry = (a.y - thy) + (l.y - tly);
         float Rz = (a.z - thz) + (l.z - tlz);
         float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
-        if (R2 >= a.w && a.w > 0.f) {
-          float vx, vy, vz;
-          seg_vel32(f4, Rx, Ry, Rz, d.x, d.y, d.z, vx, vy, vz);
+        const int id = sh_id[q][0], fw = sh_id[q][1];
+        // skip rule of calculate_vs_shift (src/tangle.c:567-569) at any
+        // distance: across a periodic face a neighbour's segment is far
+        if (fw == -1 || id == skip || fw == skip) continue;
+        float vx, vy, vz;
+        if (R2 >= a.w && seg_vel32(f4, Rx, Ry, Rz, d.x, d.y, d.z, vx, vy, vz)) {
           bx += vx; by += vy; bz += vz;
         } else {
-          int id = sh_id[q][0], fw = sh_id[q][1];
-          if (fw == -1 || id == skip || fw == skip) continue;
           const double* src = S.r1r2 + 6 * id;
           d3 v = seg_vel64(P.f4pi, mk3(src[0], src[1], src[2]), mk3(src[3], src[4], src[5]), r);
           ax += v.x; ay += v.y; az += v.z;

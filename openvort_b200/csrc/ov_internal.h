@@ -40,15 +40,15 @@ struct DevBuf {
 //   CELL_OPEN_ZERO: opening test; on failure nothing (unsplit, or every node
 //                   dropped from the children, src/octree.c:104,118-127)
 enum { CELL_LEAF1 = 0, CELL_LEAFN = 1, CELL_OPEN = 2, CELL_OPEN_P2P = 3, CELL_OPEN_ZERO = 4 };
-#define CELL_KIND_SHIFT 29
-#define CELL_SKIP_MASK ((1 << CELL_KIND_SHIFT) - 1)
 
 // One cell in depth-first preorder, one 128-byte line.  Children of cell c
 // start at c + 1; the first cell after c's subtree is `skip`.
-//   bytes   0-11  : a, b, skip | kind << 29
-//                   (LEAF1: a = node slot, b = forward slot;
-//                    otherwise a = first sorted node, b = node count)
-//   bytes  12-15  : FP32 m21
+//   bytes   0-15  : a, b, skip, meta = kind | level_top << 8 | level_bot << 16
+//                   LEAF1: a = node slot, b = forward slot
+//                   LEAFN: a = first sorted node, b = node count
+//                   OPEN*: a = FP32 m21 (bit pattern), b unused
+//                   level_top..level_bot: the octree levels the (chain of)
+//                   cell(s) spans; children start at level_bot + 1
 //   bytes  16-23  : thr, the opening test passes iff the reference-wrapped
 //                   squared distance to the centre of mass is >= thr
 //   bytes  24-47  : x = centre of mass (LEAF1: segment start r1)
@@ -56,9 +56,9 @@ enum { CELL_LEAF1 = 0, CELL_LEAFN = 1, CELL_OPEN = 2, CELL_OPEN_P2P = 3, CELL_OP
 //   bytes  72-103 : kappa/4pi * (m21, m02, m12, m22), FP64
 //   bytes 104-127 : FP32 circulation and m02, m12, m22 (the mixed form reads
 //                   bytes 0-47 and 104-127 only)
+// Node ranges of every cell (first sorted node, count) are in a side array.
 struct __align__(128) Cell {
-  int a, b, skip_kind;
-  float f_m21;
+  int a, b, skip, meta;
   double thr;
   double x[3];
   double y[3];
@@ -72,6 +72,9 @@ static_assert(offsetof(Cell, a) % 16 == 0, "int4 header load");
 static_assert(offsetof(Cell, thr) % 16 == 0, "double2 (thr, x0) load");
 static_assert(offsetof(Cell, x) % 16 == 8 && (offsetof(Cell, x) + 8) % 16 == 0, "double2 (x1, x2) load");
 static_assert(offsetof(Cell, f_g) % 8 == 0 && offsetof(Cell, f_m12) % 8 == 0, "float2 loads");
+__host__ __device__ __forceinline__ int cell_kind(int meta) { return meta & 7; }
+__host__ __device__ __forceinline__ int cell_ltop(int meta) { return (meta >> 8) & 63; }
+__host__ __device__ __forceinline__ int cell_lbot(int meta) { return (meta >> 16) & 63; }
 
 struct OvTree {
   int n_nodes = 0;      // active (non-EMPTY) nodes
@@ -83,7 +86,7 @@ struct OvTree {
   DevBuf perm;          // sorted index -> slot
   DevBuf bnode;         // binary radix tree nodes
   DevBuf cstart_cnt, cbase, cell_of;   // preorder bookkeeping
-  DevBuf cells, cell_lm;               // cell records, max box side per cell
+  DevBuf cells, cell_lm, cell_range;   // cell records, max box side, node range per cell
   DevBuf nodes64;       // per sorted node: r1 (3), r2 wrapped (3)
   DevBuf nodeids;       // per sorted node: slot, forward slot
   DevBuf nodes32;       // per sorted node: r1 - cell-free origin (FP32 not used yet)

@@ -312,6 +312,7 @@ struct CellInfo {   // per binary node (internal ids first, then leaves)
   int ltop;         // first octree level at which the range is a whole cell
   int kind;         // CELL_*
   int mac_level;    // level whose box the opening test uses (-1: none)
+  int lbot;         // last level of the chain (children start one below)
 };
 
 __device__ __forceinline__ void bnode_range(const BNode* nodes, int n, int b, int& first, int& last,
@@ -345,6 +346,7 @@ __global__ void k_classify(const BNode* __restrict__ nodes, const int* __restric
   ci.is_cell = ltop <= min(lbot, tl);
   ci.kind = CELL_LEAF1;
   ci.mac_level = -1;
+  ci.lbot = ltop;
   if (ci.is_cell) {
     int N = last - first + 1;
     // the range ends its descent inside this chain: a stop is a property of
@@ -364,6 +366,7 @@ __global__ void k_classify(const BNode* __restrict__ nodes, const int* __restric
       ci.kind = CELL_OPEN;
       ci.mac_level = lbot;
     }
+    if (ci.kind != CELL_LEAF1) ci.lbot = ci.kind == CELL_OPEN_P2P ? tl : max(ci.mac_level, ltop);
     atomicAdd(&cnt[first], 1u);
   }
   info[b] = ci;
@@ -392,8 +395,8 @@ __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __rest
                               const CellInfo* __restrict__ info, const unsigned* __restrict__ base,
                               const uint64_t* __restrict__ khi, const uint64_t* __restrict__ klo,
                               const double* __restrict__ nodes64, const int2* __restrict__ nodeids,
-                              OvParams P, int n, Cell* cells, double* cell_lm, int* lists,
-                              int* list_counts) {
+                              OvParams P, int n, Cell* cells, double* cell_lm, int2* cell_range,
+                              int* lists, int* list_counts) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= 2 * n - 1) return;
   CellInfo ci = info[b];
@@ -406,8 +409,8 @@ __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __rest
   int idx = base[first] + rank;
   Cell c;
   memset(&c, 0, sizeof(c));
-  int skip = (int)base[last + 1];
-  c.skip_kind = skip | (ci.kind << CELL_KIND_SHIFT);
+  c.skip = (int)base[last + 1];
+  c.meta = ci.kind | (ci.ltop << 8) | (ci.lbot << 16);
   c.thr = DBL_MAX;
   double Lm = 0;
   if (ci.kind == CELL_LEAF1) {
@@ -417,10 +420,11 @@ __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __rest
     c.a = id.x;
     c.b = id.y;
     for (int q = 0; q < 3; ++q) { c.x[q] = nd[q]; c.y[q] = nd[3 + q]; }
-  } else {
+  } else if (ci.kind == CELL_LEAFN) {
     c.a = first;
     c.b = last - first + 1;
   }
+  cell_range[idx] = make_int2(first, last - first + 1);
   if (ci.mac_level >= 0) {
     // replay the descent to the tested level to get the reference's box
     double lo[3] = {P.lo[0], P.lo[1], P.lo[2]}, hi[3] = {P.hi[0], P.hi[1], P.hi[2]};
@@ -468,7 +472,7 @@ __device__ __forceinline__ void write_moments(Cell* c, d3 com, d3 g, double m21,
   c->x[0] = com.x; c->x[1] = com.y; c->x[2] = com.z;
   for (int q = 0; q < 3; ++q) { c->y[q] = gs[q]; c->f_g[q] = (float)gs[q]; }
   for (int q = 0; q < 4; ++q) c->m[q] = ms[q];
-  c->f_m21 = (float)ms[0];
+  c->a = __float_as_int((float)ms[0]);
   c->f_m02 = (float)ms[1];
   c->f_m12 = (float)ms[2];
   c->f_m22 = (float)ms[3];
@@ -479,12 +483,13 @@ __device__ __forceinline__ void write_moments(Cell* c, d3 com, d3 g, double m21,
 // segment vectors; M = sum ds (x) (r - com).  Only the four entries of M the
 // expansion reads are kept.
 __global__ void k_moments_thread(const int* __restrict__ list, const int* __restrict__ list_count,
-                                 Cell* cells, const double* __restrict__ nodes64,
+                                 Cell* cells, const int2* __restrict__ cell_range,
+                                 const double* __restrict__ nodes64,
                                  const int2* __restrict__ nodeids, double f4pi) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= *list_count) return;
   int c = list[t];
-  const int start = cells[c].a, count = cells[c].b;
+  const int start = cell_range[c].x, count = cell_range[c].y;
   double sx = 0, sy = 0, sz = 0;
   for (int i = start; i < start + count; ++i) {
     const double* p = nodes64 + 6 * (size_t)i;
@@ -507,10 +512,11 @@ __global__ void k_moments_thread(const int* __restrict__ list, const int* __rest
 
 // same, one warp per cell (17..4096 nodes) or one block per cell (larger)
 template <int kThreads>
-__device__ void moments_group(int c, Cell* cells, const double* __restrict__ nodes64,
+__device__ void moments_group(int c, Cell* cells, const int2* __restrict__ cell_range,
+                              const double* __restrict__ nodes64,
                               const int2* __restrict__ nodeids, double f4pi, double* sh) {
   const int tid = kThreads == 32 ? (threadIdx.x & 31) : threadIdx.x;
-  const int start = cells[c].a, count = cells[c].b;
+  const int start = cell_range[c].x, count = cell_range[c].y;
   double s[3] = {0, 0, 0};
   for (int i = start + tid; i < start + count; i += kThreads) {
     const double* p = nodes64 + 6 * (size_t)i;
@@ -568,33 +574,37 @@ __device__ void moments_group(int c, Cell* cells, const double* __restrict__ nod
 }
 
 __global__ void k_moments_warp(const int* __restrict__ list, const int* __restrict__ list_count,
-                               Cell* cells, const double* __restrict__ nodes64,
+                               Cell* cells, const int2* __restrict__ cell_range,
+                               const double* __restrict__ nodes64,
                                const int2* __restrict__ nodeids, double f4pi) {
   int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= *list_count) return;
-  moments_group<32>(list[w], cells, nodes64, nodeids, f4pi, nullptr);
+  moments_group<32>(list[w], cells, cell_range, nodes64, nodeids, f4pi, nullptr);
 }
 
 __global__ void k_moments_block(const int* __restrict__ list, const int* __restrict__ list_count,
-                                Cell* cells, const double* __restrict__ nodes64,
+                                Cell* cells, const int2* __restrict__ cell_range,
+                                const double* __restrict__ nodes64,
                                 const int2* __restrict__ nodeids, double f4pi) {
   __shared__ double sh[264];
   if ((int)blockIdx.x >= *list_count) return;
-  moments_group<256>(list[blockIdx.x], cells, nodes64, nodeids, f4pi, sh);
+  moments_group<256>(list[blockIdx.x], cells, cell_range, nodes64, nodeids, f4pi, sh);
 }
 
 // a tangle of one node: the root is that node's leaf
-__global__ void k_single_cell(Cell* cells, double* cell_lm, const double* __restrict__ nodes64,
-                              const int2* __restrict__ nodeids) {
+__global__ void k_single_cell(Cell* cells, double* cell_lm, int2* cell_range,
+                              const double* __restrict__ nodes64, const int2* __restrict__ nodeids) {
   Cell c;
   memset(&c, 0, sizeof(c));
   c.a = nodeids[0].x;
   c.b = nodeids[0].y;
-  c.skip_kind = 1 | (CELL_LEAF1 << CELL_KIND_SHIFT);
+  c.skip = 1;
+  c.meta = CELL_LEAF1;
   c.thr = DBL_MAX;
   for (int q = 0; q < 3; ++q) { c.x[q] = nodes64[q]; c.y[q] = nodes64[3 + q]; }
   cells[0] = c;
   cell_lm[0] = 0;
+  cell_range[0] = make_int2(0, 1);
 }
 
 }  // namespace
@@ -603,7 +613,7 @@ __global__ void k_single_cell(Cell* cells, double* cell_lm, const double* __rest
 void ov_tree_release(OvTree* t) {
   DevBuf* bufs[] = {&t->keys, &t->keys_alt, &t->vals, &t->vals_alt, &t->stop, &t->hist,
                     &t->perm, &t->bnode, &t->cstart_cnt, &t->cbase, &t->cell_of, &t->cells,
-                    &t->cell_lm, &t->nodes64, &t->nodeids, &t->nodes32, &t->counters,
+                    &t->cell_lm, &t->cell_range, &t->nodes64, &t->nodeids, &t->nodes32, &t->counters,
                     &t->scratch};
   for (DevBuf* b : bufs) b->release();
   t->n_nodes = t->n_cells = t->built = 0;
@@ -707,6 +717,7 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
       !T->cbase.reserve(sizeof(unsigned) * (size_t)(na + 1)) ||
       !T->cells.reserve(sizeof(Cell) * (size_t)nbin) ||
       !T->cell_lm.reserve(sizeof(double) * (size_t)nbin) ||
+      !T->cell_range.reserve(sizeof(int2) * (size_t)nbin) ||
       !T->cell_of.reserve(sizeof(int) * (3 * 2 * (size_t)na) + 64))
     return false;
   BNode* bn = T->bnode.as<BNode>();
@@ -718,8 +729,10 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
   int* list_counts = ctr + 4;
   Cell* cells = T->cells.as<Cell>();
   double* cell_lm = T->cell_lm.as<double>();
+  int2* cell_range = T->cell_range.as<int2>();
   if (na == 1) {
-    k_single_cell<<<1, 1, 0, st>>>(cells, cell_lm, T->nodes64.as<double>(), T->nodeids.as<int2>());
+    k_single_cell<<<1, 1, 0, st>>>(cells, cell_lm, cell_range, T->nodes64.as<double>(),
+                                   T->nodeids.as<int2>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
     T->n_cells = 1;
@@ -733,7 +746,8 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     OV_LAUNCHED();
     k_write_cells<<<(nbin + 255) / 256, 256, 0, st>>>(bn, leaf_parent, info, base, hi_sorted, klo,
                                                       T->nodes64.as<double>(), T->nodeids.as<int2>(),
-                                                      s->P, na, cells, cell_lm, lists, list_counts);
+                                                      s->P, na, cells, cell_lm, cell_range, lists,
+                                                      list_counts);
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
     unsigned nc = 0;
@@ -744,18 +758,18 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     T->n_cells = (int)nc;
     const double f4 = s->P.f4pi;
     if (lc[0] > 0) {
-      k_moments_thread<<<(lc[0] + 127) / 128, 128, 0, st>>>(lists, list_counts, cells,
+      k_moments_thread<<<(lc[0] + 127) / 128, 128, 0, st>>>(lists, list_counts, cells, cell_range,
                                                             T->nodes64.as<double>(), T->nodeids.as<int2>(), f4);
       OV_LAUNCHED();
     }
     if (lc[1] > 0) {
       k_moments_warp<<<(lc[1] * 32 + 255) / 256, 256, 0, st>>>(lists + 2 * (size_t)na, list_counts + 1,
-                                                              cells, T->nodes64.as<double>(),
+                                                              cells, cell_range, T->nodes64.as<double>(),
                                                               T->nodeids.as<int2>(), f4);
       OV_LAUNCHED();
     }
     if (lc[2] > 0) {
-      k_moments_block<<<lc[2], 256, 0, st>>>(lists + 4 * (size_t)na, list_counts + 2, cells,
+      k_moments_block<<<lc[2], 256, 0, st>>>(lists + 4 * (size_t)na, list_counts + 2, cells, cell_range,
                                              T->nodes64.as<double>(), T->nodeids.as<int2>(), f4);
       OV_LAUNCHED();
     }

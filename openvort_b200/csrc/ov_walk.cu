@@ -28,6 +28,7 @@ namespace {
 struct TreeView {
   const Cell* cells;
   const double* cell_lm;   // max box side per cell (opening test at a user theta)
+  const int2* cell_range;  // first sorted node and count per cell
   const double* nodes64;   // per sorted node: r1, wrapped r2
   const int2* nodeids;     // per sorted node: slot, forward slot
   int n_cells;
@@ -103,10 +104,10 @@ __device__ __forceinline__ void p2p_one(const OvParams& P, d3 r1, d3 r2, d3 rp, 
     d3 R = r1 - rp;
     d3 ds = r2 - r1;
     double R2 = dot3(R, R), ds2 = dot3(ds, ds);
-    if (R2 >= 16.0 * ds2 && ds2 > 0) {
-      float vx, vy, vz;
-      seg_vel32((float)P.f4pi, (float)R.x, (float)R.y, (float)R.z, (float)ds.x, (float)ds.y,
-                (float)ds.z, vx, vy, vz);
+    float vx, vy, vz;
+    if (R2 >= 16.0 * ds2 && ds2 > 0 &&
+        seg_vel32((float)P.f4pi, (float)R.x, (float)R.y, (float)R.z, (float)ds.x, (float)ds.y,
+                  (float)ds.z, vx, vy, vz)) {
       ax += vx; ay += vy; az += vz;
       return;
     }
@@ -131,11 +132,11 @@ __device__ d3 warp_walk(const OvParams& P, const TreeView& T, d3 rp, bool live, 
     if (q >= T.n_cells) break;
     const Cell* cp = T.cells + q;
     if (lane == 0 && q + 1 < T.n_cells) prefetch_l1(cp + 1);
-    const int4 h = *reinterpret_cast<const int4*>(cp);           // a, b, skip|kind, f_m21
+    const int4 h = *reinterpret_cast<const int4*>(cp);              // a, b, skip, meta
     const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);  // thr, x0
     const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]); // x1, x2
-    const int kind = (unsigned)h.z >> CELL_KIND_SHIFT;
-    const int skp = h.z & CELL_SKIP_MASK;
+    const int kind = cell_kind(h.w);
+    const int skp = h.z;
     if (lane == 1 && skp < T.n_cells) prefetch_l1(T.cells + skp);
     int act = ACT_NONE;
     if (next == q) {
@@ -162,7 +163,7 @@ __device__ d3 warp_walk(const OvParams& P, const TreeView& T, d3 rp, bool live, 
         const float2 f1 = *reinterpret_cast<const float2*>(&cp->f_g[2]);  // g2 m02
         const float2 f2 = *reinterpret_cast<const float2*>(&cp->f_m12);   // m12 m22
         float vx, vy, vz;
-        expansion32(f0.x, f0.y, f1.x, __int_as_float(h.w), f1.y, f2.x, f2.y, (float)(rp.x - t0.y),
+        expansion32(f0.x, f0.y, f1.x, __int_as_float(h.x), f1.y, f2.x, f2.y, (float)(rp.x - t0.y),
                     (float)(rp.y - t1.x), (float)(rp.z - t1.y), vx, vy, vz);
         ax += vx; ay += vy; az += vz;
       } else {
@@ -183,9 +184,10 @@ __device__ d3 warp_walk(const OvParams& P, const TreeView& T, d3 rp, bool live, 
       ++n_iter;
     }
     if (pn_mask) {
-      const int end = min(h.x + h.y, T.n_nodes);
-      if (lane == 0) n_p2p += (unsigned long long)__popc(pn_mask) * h.y;
-      for (int i = max(h.x, 0); i < end; ++i) {
+      const int2 rg = T.cell_range[q];
+      const int end = min(rg.x + rg.y, T.n_nodes);
+      if (lane == 0) n_p2p += (unsigned long long)__popc(pn_mask) * rg.y;
+      for (int i = max(rg.x, 0); i < end; ++i) {
         const int2 id = T.nodeids[i];
         if (act != ACT_P2PN) continue;
         if (id.y == -1 || id.x == skip || id.y == skip) continue;
@@ -195,6 +197,267 @@ __device__ d3 warp_walk(const OvParams& P, const TreeView& T, d3 rp, bool live, 
     }
   }
   return mk3(ax, ay, az);
+}
+
+// ----------------------------------------------------------------------
+// Multi-image walk (tables of periodic shifts in {-1,0,1}^3, no mirrors).
+//
+// The reference walks the tree once per image point r - L s (27 walks for
+// periodic-26), each with its own opening decisions, because the opening
+// distance is |r - L s - com| after a single box wrap of the centre of mass
+// (src/octree.c:286).  Per axis that distance is the minimum image for s = 0
+// and either the same value or a larger one for s = +-1, so every image's
+// walk visits a subset of the cells of the s = 0 walk.  One traversal per
+// target therefore serves all images: each lane keeps, per tree level, the
+// 27-bit mask of images that opened the parent, makes each image's decision
+// exactly as the reference would (per-axis wrapped distances with its FP64
+// operations), evaluates every image that accepts the cell or reaches a leaf
+// from the same cell load, and descends while any image opens.
+//
+// combo c = 9 (sx+1) + 3 (sy+1) + (sz+1); c = 13 is the tangle itself.
+
+constexpr int kCombos = 27;
+constexpr int kPrimary = 13;
+constexpr int kLevelSlots = 34;
+constexpr int kMultiWarps = 4;
+
+// wrapped component u and its square for one image coordinate v
+__device__ __forceinline__ double wrapped_sq(const OvParams& P, int a, double v, double c) {
+  double cc = c;
+  if (P.periodic[a]) {
+    double d = __dsub_rn(c, v);
+    if (d > P.L[a] * 0.5) cc = __dsub_rn(c, P.L[a]);
+    else if (d < -P.L[a] * 0.5) cc = __dadd_rn(c, P.L[a]);
+  }
+  double u = __dsub_rn(v, cc);
+  return __dmul_rn(u, u);
+}
+
+__device__ __forceinline__ double sel3(int i, double a, double b, double c) {
+  return i == 0 ? a : (i == 1 ? b : c);
+}
+__device__ __forceinline__ float sel3f(int i, float a, float b, float c) {
+  return i == 0 ? a : (i == 1 ? b : c);
+}
+
+// FP64 reference formula for one segment at one image point, out of line so
+// the image loops stay small in the instruction cache
+__device__ __forceinline__ d3 seg64_at(double f4pi, d3 r1, d3 r2, d3 t) { return seg_vel64(f4pi, r1, r2, t); }
+__device__ __forceinline__ d3 expansion64_at(const Cell* cp, d3 R) { return expansion64(cp->y, cp->m, R); }
+
+// One segment r1 -> r2 for every image in `mask`: FP64 with the reference's
+// cut-offs and skip rule (the skip applies to the tangle itself only), or in
+// the mixed form FP32 beyond the near radius.  Images are visited as nine
+// (x, y) columns of three z shifts, the z loop unrolled.
+// image coordinate r - L s along one axis, s = i - 1, with the reference's
+// single rounding (shifted, src/tangle.c:51-53)
+__device__ __forceinline__ double img_coord(double r, double L, int i) {
+  return i == 1 ? r : (i == 0 ? __dsub_rn(r, -L) : __dsub_rn(r, L));
+}
+
+template <bool kMixed>
+__device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 r, d3 r1, d3 r2,
+                                           int id, int fw, int skip, double near2, d3& nl, d3& im,
+                                           unsigned& n_p2p) {
+  if (fw == -1) return;
+  if (id == skip || fw == skip) mask &= ~(1u << kPrimary);
+  n_p2p += __popc(mask);
+  const d3 ds = r2 - r1;
+  const double ds2 = dot3(ds, ds);
+  const double far2 = fmax(16.0 * ds2, near2);
+  const float dsx = (float)ds.x, dsy = (float)ds.y, dsz = (float)ds.z;
+  const float f4 = (float)P.f4pi;
+  float fx = 0, fy = 0, fz = 0;
+  // one image per iteration, rolled: a single copy of each formula
+#pragma unroll 1
+  while (mask) {
+    const int c = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const int ix = (c * 57) >> 9, rem = c - 9 * ix, iy = (rem * 11) >> 5, iz = rem - 3 * iy;
+    const d3 t = mk3(img_coord(r.x, P.L[0], ix), img_coord(r.y, P.L[1], iy), img_coord(r.z, P.L[2], iz));
+    if (kMixed) {
+      const d3 R = r1 - t;
+      const double R2 = dot3(R, R);
+      float vx, vy, vz;
+      if (R2 >= far2 && ds2 > 0 &&
+          seg_vel32(f4, (float)R.x, (float)R.y, (float)R.z, dsx, dsy, dsz, vx, vy, vz)) {
+        if (c == kPrimary) nl = nl + mk3(vx, vy, vz);
+        else { fx += vx; fy += vy; fz += vz; }
+        continue;
+      }
+    }
+    const d3 v = seg64_at(P.f4pi, r1, r2, t);
+    if (c == kPrimary) nl = nl + v;
+    else im = im + v;
+  }
+  if (kMixed) im = im + mk3(fx, fy, fz);
+}
+
+template <bool kMixed>
+__global__ void __launch_bounds__(kMultiWarps * 32) k_walk_multi(
+    OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
+    const double* __restrict__ pos, int n_t, unsigned combos, double near2, double* v_nl,
+    double* v_img, unsigned long long* counters) {
+  __shared__ unsigned sh_mask[kMultiWarps][kLevelSlots][32];
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kMultiWarps + warp;
+  if (gw * 32 >= n_t) return;   // whole warp out of range
+  const int i = gw * 32 + lane;
+  const int k = i < n_t ? (order ? order[i] : i) : -1;
+  const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
+  const d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
+  unsigned* lvl_mask = &sh_mask[warp][0][lane];   // level l at lvl_mask[32 l]
+  lvl_mask[0] = combos;
+  d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
+  unsigned n_p2p = 0, n_far = 0, n_iter = 0;
+  int next = live ? 0 : T.n_cells;
+  __syncwarp();
+  for (;;) {
+    const int q = (int)__reduce_min_sync(FULL, (unsigned)next);
+    if (q >= T.n_cells) break;
+    const Cell* cp = T.cells + q;
+    if (lane == 0 && q + 1 < T.n_cells) prefetch_l1(cp + 1);
+    const int4 h = *reinterpret_cast<const int4*>(cp);
+    const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);
+    const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]);
+    const int kind = cell_kind(h.w);
+    if (lane == 1 && h.z < T.n_cells) prefetch_l1(T.cells + h.z);
+    unsigned p2p_mask = 0;   // images summing this cell's node range directly
+    if (next == q) {
+      const unsigned m = lvl_mask[32 * cell_ltop(h.w)];
+      unsigned open = 0;
+      if (kind == CELL_LEAF1) {
+        p2p_images<kMixed>(P, m, r, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x,
+                           h.y, k, near2, nl, im, n_p2p);
+      } else if (kind == CELL_LEAFN) {
+        p2p_mask = m;
+      } else {
+        // opening test per image (octree_get_vs, src/octree.c:284-296): the
+        // wrapped squared distance, summed x + y then + z as the reference does
+        const double cx = t0.y, cy = t1.x, cz = t1.y;
+        const double qx[3] = {wrapped_sq(P, 0, img_coord(r.x, P.L[0], 0), cx), wrapped_sq(P, 0, r.x, cx),
+                              wrapped_sq(P, 0, img_coord(r.x, P.L[0], 2), cx)};
+        const double qy[3] = {wrapped_sq(P, 1, img_coord(r.y, P.L[1], 0), cy), wrapped_sq(P, 1, r.y, cy),
+                              wrapped_sq(P, 1, img_coord(r.y, P.L[1], 2), cy)};
+        const double qz[3] = {wrapped_sq(P, 2, img_coord(r.z, P.L[2], 0), cz), wrapped_sq(P, 2, r.z, cz),
+                              wrapped_sq(P, 2, img_coord(r.z, P.L[2], 2), cz)};
+        unsigned pass = 0;
+#pragma unroll 1
+        for (int xy = 0; xy < 9; ++xy) {
+          if (!(m & (7u << (3 * xy)))) continue;
+          const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
+          const double qxy = __dadd_rn(sel3(ix, qx[0], qx[1], qx[2]), sel3(iy, qy[0], qy[1], qy[2]));
+#pragma unroll
+          for (int iz = 0; iz < 3; ++iz)
+            if (__dadd_rn(qxy, qz[iz]) >= t0.x) pass |= 1u << (3 * xy + iz);
+        }
+        pass &= m;
+        const unsigned fail = m & ~pass;
+        if (kind == CELL_OPEN) open = fail;
+        else if (kind == CELL_OPEN_P2P) p2p_mask = fail;
+        if (pass) {
+          n_far += __popc(pass);
+          // expansion at every accepting image: R = r - L s - com, unwrapped
+          if (kMixed) {
+            const float2 f0 = *reinterpret_cast<const float2*>(&cp->f_g[0]);
+            const float2 f1 = *reinterpret_cast<const float2*>(&cp->f_g[2]);
+            const float2 f2 = *reinterpret_cast<const float2*>(&cp->f_m12);
+            const float m21 = __int_as_float(h.x);
+            // FP32 copies of the FP64-formed offsets per axis and shift
+            const float Fx0 = (float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
+                        Fx1 = (float)__dsub_rn(r.x, cx),
+                        Fx2 = (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx);
+            const float Fy0 = (float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
+                        Fy1 = (float)__dsub_rn(r.y, cy),
+                        Fy2 = (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy);
+            const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
+                                 (float)__dsub_rn(r.z, cz),
+                                 (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+            const float fnear2 = (float)near2;
+            float ax = 0, ay = 0, az = 0;
+#pragma unroll 1
+            for (int xy = 0; xy < 9; ++xy) {
+              const unsigned bits = (pass >> (3 * xy)) & 7u;
+              if (!bits) continue;
+              const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
+              const float X = sel3f(ix, Fx0, Fx1, Fx2);
+              const float Y = sel3f(iy, Fy0, Fy1, Fy2);
+#pragma unroll
+              for (int iz = 0; iz < 3; ++iz) {
+                if (!((bits >> iz) & 1u)) continue;
+                const int c = 3 * xy + iz;
+                const float Z = Fz[iz];
+                if (fmaf(X, X, fmaf(Y, Y, Z * Z)) < fnear2) {
+                  // near field: FP64 expansion from the FP64 offsets
+                  const d3 v = expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ix), cx),
+                                                      __dsub_rn(img_coord(r.y, P.L[1], iy), cy),
+                                                      __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
+                  if (c == kPrimary) nl = nl + v; else im = im + v;
+                  continue;
+                }
+                float vx, vy, vz;
+                expansion32(f0.x, f0.y, f1.x, m21, f1.y, f2.x, f2.y, X, Y, Z, vx, vy, vz);
+                if (c == kPrimary) nl = nl + mk3(vx, vy, vz);
+                else { ax += vx; ay += vy; az += vz; }
+              }
+            }
+            im = im + mk3(ax, ay, az);
+          } else {
+            const double g[3] = {cp->y[0], cp->y[1], cp->y[2]};
+            const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
+            const double Rz[3] = {__dsub_rn(img_coord(r.z, P.L[2], 0), cz), __dsub_rn(r.z, cz),
+                                  __dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+#pragma unroll 1
+            for (int xy = 0; xy < 9; ++xy) {
+              const unsigned bits = (pass >> (3 * xy)) & 7u;
+              if (!bits) continue;
+              const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
+              const double X = __dsub_rn(img_coord(r.x, P.L[0], ix), cx);
+              const double Y = __dsub_rn(img_coord(r.y, P.L[1], iy), cy);
+#pragma unroll
+              for (int iz = 0; iz < 3; ++iz) {
+                if (!((bits >> iz) & 1u)) continue;
+                const d3 v = expansion64(g, mm, mk3(X, Y, Rz[iz]));
+                if (3 * xy + iz == kPrimary) nl = nl + v; else im = im + v;
+              }
+            }
+          }
+        }
+      }
+      if (open) lvl_mask[32 * (cell_lbot(h.w) + 1)] = open;
+      // each lane's next cell strictly increases: the loop ends within n_cells
+      next = open ? q + 1 : max(h.z, q + 1);
+    }
+    ++n_iter;
+    // direct sums over a node range (grain leaves), shared by the warp
+    if (__ballot_sync(FULL, p2p_mask != 0)) {
+      const int2 rg = T.cell_range[q];
+      const int end = min(rg.x + rg.y, T.n_nodes);
+      for (int j = max(rg.x, 0); j < end; ++j) {
+        const int2 id = T.nodeids[j];
+        if (!p2p_mask) continue;
+        const double* nd = T.nodes64 + 6 * (size_t)j;
+        p2p_images<kMixed>(P, p2p_mask, r, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), id.x,
+                           id.y, k, near2, nl, im, n_p2p);
+      }
+    }
+  }
+  if (live) {
+    st3(v_nl, k, nl);
+    st3(v_img, k, im);
+  }
+  // counters: per-warp sums
+  unsigned long long a = n_p2p, b = n_far;
+  for (int off = 16; off > 0; off >>= 1) {
+    a += __shfl_xor_sync(FULL, a, off);
+    b += __shfl_xor_sync(FULL, b, off);
+  }
+  if (lane == 0) {
+    atomicAdd(&counters[0], a);
+    atomicAdd(&counters[1], b);
+    atomicAdd(&counters[2], (unsigned long long)n_iter);
+  }
 }
 
 // All nodes: warp w handles sorted targets 32w .. 32w+31, every image.
@@ -272,6 +535,7 @@ TreeView view_of(OvTree* t) {
   TreeView v;
   v.cells = t->cells.as<Cell>();
   v.cell_lm = t->cell_lm.as<double>();
+  v.cell_range = t->cell_range.as<int2>();
   v.nodes64 = t->nodes64.as<double>();
   v.nodeids = t->nodeids.as<int2>();
   v.n_cells = t->n_cells;
@@ -305,24 +569,55 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
     OV_TRY_CUDA(cudaMemsetAsync(v_img, 0, sizeof(double) * 3 * s->n, s->stream));
     return true;
   }
-  int warps = (n_t + 31) / 32;
-  int blocks = (warps * 32 + 127) / 128;
   TreeView tv = view_of(t);
   OvParams P = t->P;
   // image table and precision of this call; geometry of the tree's build
   P.n_img = s->P.n_img;
   for (int j = 0; j < P.n_img; ++j)
     for (int c = 0; c < 4; ++c) P.img[j][c] = s->P.img[j][c];
-  cudaEventRecord(s->ev1, s->stream);
-  if (s->P.precision == OV_PREC_MIXED) {
-    k_walk_nodes<true><<<blocks, 128, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos, n_t,
-                                                       v_nl, v_img, ctr);
-    OV_LAUNCHED();
+  P.precision = s->P.precision;
+  const bool mixed = s->P.precision == OV_PREC_MIXED;
+  // images as a set of periodic shifts in {-1,0,1}^3 without mirrors or
+  // repeats: one multi-image walk per target
+  unsigned combos = 1u << 13;
+  bool multi = true;
+  for (int j = 0; j < P.n_img && multi; ++j) {
+    const int* im = P.img[j];
+    if (im[3] != -1 || im[0] < -1 || im[0] > 1 || im[1] < -1 || im[1] > 1 || im[2] < -1 ||
+        im[2] > 1) {
+      multi = false;
+      break;
+    }
+    unsigned bit = 1u << (9 * (im[0] + 1) + 3 * (im[1] + 1) + (im[2] + 1));
+    if (combos & bit) multi = false;
+    combos |= bit;
   }
-  else {
-    k_walk_nodes<false><<<blocks, 128, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos, n_t,
-                                                        v_nl, v_img, ctr);
-    OV_LAUNCHED();
+  const double near2 = s->P.near2;
+  cudaEventRecord(s->ev1, s->stream);
+  if (multi) {
+    int warps = (n_t + 31) / 32;
+    int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
+    if (mixed) {
+      k_walk_multi<true><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
+      OV_LAUNCHED();
+    } else {
+      k_walk_multi<false><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
+      OV_LAUNCHED();
+    }
+  } else {
+    int warps = (n_t + 31) / 32;
+    int blocks = (warps * 32 + 127) / 128;
+    if (mixed) {
+      k_walk_nodes<true><<<blocks, 128, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos, n_t,
+                                                         v_nl, v_img, ctr);
+      OV_LAUNCHED();
+    } else {
+      k_walk_nodes<false><<<blocks, 128, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos, n_t,
+                                                          v_nl, v_img, ctr);
+      OV_LAUNCHED();
+    }
   }
   OV_TRY_CUDA(cudaGetLastError());
   cudaEventRecord(s->ev2, s->stream);
