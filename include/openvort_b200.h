@@ -291,6 +291,36 @@ typedef struct {
 int ov_state_get_stats(ov_state *s, ov_run_stats *out);
 void ov_state_reset_stats(ov_state *s);
 
+/* Direct Biot-Savart velocity (the tangle's own segments plus the boundary
+ * image sum, as ov_state_eval_points with method 0) at npts points, for
+ * callers that cannot call cudaMalloc: code whose device memory is owned by
+ * another framework's allocator, or a loop that must not allocate.  It
+ * allocates nothing: inputs and outputs are the caller's device buffers and
+ * the scratch (segment table and per-image partial sums) is one file-scope
+ * device array of fixed size that every GPU loading this library holds
+ * until the process exits.  No counterpart in the reference.
+ *   header   host tangle header: only N, box and bimg are read
+ *   d_pos    3*N doubles, d_links 2*N ints (forward, reverse), d_status
+ *            2*N ints (status, pin wall), all device memory
+ *   d_pts    3*npts doubles, d_skip npts ints or NULL (node skipped in the
+ *            tangle's own sum), d_out 3*npts doubles, all device memory
+ *   stream   a cudaStream_t (NULL: the default stream); the call only
+ *            enqueues work on it and returns
+ * Limits: N <= OV_NOALLOC_MAX_NODES, npts <= OV_NOALLOC_MAX_POINTS and
+ * npts * (1 + bimg.n) <= OV_NOALLOC_MAX_POINT_IMAGES; larger sizes return
+ * OV_ERR_INVALID.  The first call on each device looks up the array's device
+ * address (cudaGetSymbolAddress) with that device current; make that first
+ * call before any stream capture.  All calls share the one array, which
+ * keeps the last call's contents: calls whose work overlaps on the GPU (on
+ * different streams, or host threads) race. */
+#define OV_NOALLOC_MAX_NODES 131072
+#define OV_NOALLOC_MAX_POINTS 131072
+#define OV_NOALLOC_MAX_POINT_IMAGES 131072
+int ov_direct_points_noalloc(const struct tangle_state *header, const double *d_pos,
+                             const int *d_links, const int *d_status, int npts,
+                             const double *d_pts, const int *d_skip, double *d_out,
+                             void *stream);
+
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);

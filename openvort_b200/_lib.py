@@ -29,7 +29,7 @@ FUNCTIONS = [
     "ov_state_create", "ov_state_destroy", "ov_state_upload", "ov_state_download",
     "ov_state_update_tangle", "ov_state_rk4_step", "ov_state_run", "ov_state_eval_points",
     "ov_measure_fma_peak", "ov_state_get_stats", "ov_state_reset_stats",
-    "ov_set_mixed_near_factor", "ov_get_mixed_near_factor",
+    "ov_set_mixed_near_factor", "ov_get_mixed_near_factor", "ov_direct_points_noalloc",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -111,6 +111,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_state_reset_stats": (None, [C.c_void_p]),
         "ov_set_mixed_near_factor": (None, [C.c_double]),
         "ov_get_mixed_near_factor": (C.c_double, []),
+        "ov_direct_points_noalloc": (C.c_int, [T, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                               C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

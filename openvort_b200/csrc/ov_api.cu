@@ -367,6 +367,12 @@ bool capture_params(const tangle_state* t, OvParams& P, bool need_flows) {
 
 }  // namespace
 
+// Box, image table and globals of a tangle header (no flows, no node arrays
+// read): the parameters of a point query.
+bool ov_capture_header_params(const struct tangle_state* t, OvParams& P) {
+  return capture_params(t, P, false);
+}
+
 // ======================================================================
 // state management
 

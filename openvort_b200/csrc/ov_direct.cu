@@ -303,3 +303,26 @@ bool ov_add3(cudaStream_t st, const double* a, const double* b, double* out, int
   OV_TRY_CUDA(cudaGetLastError());
   return true;
 }
+
+// The direct point query with caller-provided scratch (ov_noalloc.cu):
+// segment table seg (6 doubles per node) and fwd (n ints), per-image partial
+// sums part (3 doubles per point and image), image sums img (3 per point).
+// Launches only, on `st`; out = the tangle's own sum + the image sum.
+bool ov_direct_points_scratch(cudaStream_t st, const OvParams& P, const double* pos,
+                              const int2* links, const int2* status, int n, int npts,
+                              const double* pts, const int* skip, double* seg, int* fwd,
+                              double* part, double* out, double* img) {
+  if (n > 0) {
+    k_segtab<<<(n + 255) / 256, 256, 0, st>>>(P, pos, links, status, seg, fwd, n);
+    OV_LAUNCHED();
+  }
+  dim3 grid((npts + kTB - 1) / kTB, P.n_img + 1);
+  k_direct64<<<grid, kTB, 0, st>>>(P, SegTab{seg, fwd}, n, nullptr, pts, nullptr, skip, npts, part);
+  OV_LAUNCHED();
+  k_reduce_images<<<(npts + 255) / 256, 256, 0, st>>>(P, part, npts, out, img);
+  OV_LAUNCHED();
+  k_add3<<<(3 * npts + 255) / 256, 256, 0, st>>>(out, img, out, npts);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}

@@ -153,6 +153,11 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
 bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const double* pts,
                       const int* skip, const int* only, int n_only, double* out_nl,
                       double* out_img);
+// direct point query on caller-provided scratch (see ov_direct.cu)
+bool ov_direct_points_scratch(cudaStream_t st, const OvParams& P, const double* pos,
+                              const int2* links, const int2* status, int n, int npts,
+                              const double* pts, const int* skip, double* seg, int* fwd,
+                              double* part, double* out, double* img);
 // out = a + b for n vectors of 3 doubles (device)
 bool ov_add3(cudaStream_t st, const double* a, const double* b, double* out, int n);
 
