@@ -44,7 +44,19 @@ UNIT = "point-velocity evals/s"
 D = 0.4
 DL = D / 800
 FLOPS_P2P = 43.0   # per segment-point interaction (direct sum / tree leaves)
+
+
+def _hbm_peak():
+    """Measured copy bandwidth of this GPU model (GB/s), else 6650 (fallback)."""
+    try:
+        return float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+HBM_PEAK, HBM_PEAK_SOURCE = _hbm_peak()
 FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
+WALK_DRAM_BYTES_PER_POINT = None  # dram__bytes_read.sum + dram__bytes_write.sum / points, ncu
 
 
 def parse():
@@ -371,14 +383,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(tangle, p, target_s=10.0)
 
-    traffic = None
-    tfile = ROOT / "profiles" / "bh_walk_traffic.json"
-    if tfile.exists():
-        try:
-            tr = json.loads(tfile.read_text())
-            traffic = tr["dram_bytes_per_launch_per_point"] * n
-        except Exception:
-            traffic = None
+    # DRAM bytes (read + write) per walk launch, from the ncu capture of this
+    # kernel on this workload, scaled by the points per launch
+    traffic = WALK_DRAM_BYTES_PER_POINT * n if WALK_DRAM_BYTES_PER_POINT else None
 
     if rank == 0:
         line = {
@@ -399,12 +406,17 @@ def main():
             **err,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32.value, "unit": "TFLOP/s",
                          "frac": achieved / peak32.value if peak32.value else None, "traffic": traffic,
-                         "kernel": "k_walk_nodes<mixed> (Barnes-Hut walk, 27 walks per point)",
+                         "kernel": "k_walk_multi<mixed> (Barnes-Hut walk, one traversal per point for all 27 images)",
                          "peak_source": "ov_measure_fma_peak: FP32 FMA burst on this GPU, this run",
                          "flops_per_launch": flops / max(1.0, rs.bs_launches),
                          "launch_ms": walk_ms, "share_of_step": walk_share,
-                         "walk_lane_utilization": (rs.interactions + rs.cell_interactions) /
-                                                  max(1.0, 32.0 * rs.warp_iterations),
+                         "p2p_interactions_per_point": rs.interactions / max(1.0, rs.bs_launches) / n,
+                         "cell_interactions_per_point": rs.cell_interactions / max(1.0, rs.bs_launches) / n,
+                         "cell_visits_per_warp": rs.warp_iterations / max(1.0, rs.bs_launches) / (n / 32.0),
+                         "hbm": ({"achieved_gbs": traffic / (walk_ms / 1e3) / 1e9, "peak_gbs": HBM_PEAK,
+                                  "frac": traffic / (walk_ms / 1e3) / 1e9 / HBM_PEAK,
+                                  "peak_source": HBM_PEAK_SOURCE + " copy bandwidth"}
+                                 if traffic else None),
                          "tree_build_share_of_step": build_share},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -321,6 +321,64 @@ int ov_direct_points_noalloc(const struct tangle_state *header, const double *d_
                              const double *d_pts, const int *d_skip, double *d_out,
                              void *stream);
 
+/* ----- batched ensembles of independent systems -----
+ * Many small open-boundary systems (each a few closed loops) advanced
+ * together: the reference runs one tangle per process, so this has no
+ * counterpart there.  Every system evolves exactly as a tangle of its own
+ * would under update_tangle + rk4_step: its velocity sums only its own
+ * segments (direct Biot-Savart, no tree, no images); local induction,
+ * external flows, hyperfriction and mutual friction are per node as usual.
+ *   all      one tangle_state holding every system's slots, system s in
+ *            slots offsets[s] .. offsets[s+1]-1; every link stays inside its
+ *            system; all six walls open, no boundary images
+ *   offsets  n_systems + 1 non-decreasing slot offsets, offsets[0] = 0,
+ *            offsets[n_systems] = all->N
+ * The globals and flows are read at create and at every run/update call;
+ * ov_set_precision selects FP64 or the mixed form (FP32 beyond the near
+ * radius, which here is the near factor times each system's own longest
+ * segment).  The Biot-Savart sum of all systems is one persistent kernel
+ * per RK4 stage that takes (system, block of targets) work items, largest
+ * systems first; ov_batch_run captures one RK4 step in a CUDA graph and
+ * replays it. */
+typedef struct ov_batch ov_batch;
+ov_batch *ov_batch_create(const struct tangle_state *all, int n_systems, const int *offsets);
+void ov_batch_destroy(ov_batch *b);
+/* one velocity evaluation (update_tangle) at the current positions */
+int ov_batch_update(ov_batch *b, double t);
+/* nsteps x (update_tangle + rk4_step) at t0, t0 + dt, ..., as one CUDA
+ * graph per RK4 step, replayed */
+int ov_batch_run(ov_batch *b, double t0, double dt, int nsteps);
+/* copy results of every system out (OV_FIELD_* mask) */
+int ov_batch_download(ov_batch *b, struct tangle_state *all, int what);
+/* Biot-Savart kernel shape: targets per block (64, 128 or 256), sources
+ * per shared-memory tile (64, 128 or 256) and resident blocks per SM of the
+ * persistent grid (0: as many as fit).  ov_batch_autotune times the
+ * candidates on the batch's own systems and keeps the fastest. */
+typedef struct {
+  int targets_per_block;
+  int sources_per_tile;
+  int blocks_per_sm;
+  double kernel_ms;   /* device time of one Biot-Savart launch (autotune) */
+} ov_batch_tuning;
+int ov_batch_set_tuning(ov_batch *b, const ov_batch_tuning *tuning);
+int ov_batch_get_tuning(ov_batch *b, ov_batch_tuning *out);
+int ov_batch_autotune(ov_batch *b, ov_batch_tuning *out);
+/* counters: evaluations and segment-point interactions since creation,
+ * device time of the last run, average device time of the Biot-Savart
+ * launches of the last RK4 step (or of the last update), kernels per RK4
+ * step, and the ensemble's targets, segments and systems */
+typedef struct {
+  double evals;
+  double interactions;
+  double last_run_ms;
+  double bs_kernel_ms;
+  double kernels_per_step;
+  double n_targets;
+  double n_segments;
+  double n_systems;
+} ov_batch_stats;
+int ov_batch_get_stats(ov_batch *b, ov_batch_stats *out);
+
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);

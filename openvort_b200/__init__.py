@@ -129,3 +129,62 @@ class DeviceState:
             self.close()
         except Exception:
             pass
+
+
+class DeviceBatch:
+    """An ensemble of independent open-boundary systems resident in device
+    memory (ov_batch_*): system s occupies slots offsets[s] .. offsets[s+1]-1
+    of the one HostTangle `t`."""
+
+    def __init__(self, t: HostTangle, offsets):
+        self.lib = load()
+        self.t = t
+        self.offsets = np.ascontiguousarray(offsets, dtype=np.int32)
+        self.h = self.lib.ov_batch_create(t.ptr(), len(self.offsets) - 1, self.offsets.ctypes.data)
+        if not self.h:
+            check(self.lib)
+            raise OVError(1, "ov_batch_create failed")
+
+    def _rc(self, rc):
+        if rc != 0:
+            check(self.lib)
+            raise OVError(rc, "call failed")
+
+    def update(self, time: float = 0.0):
+        self._rc(self.lib.ov_batch_update(self.h, time))
+
+    def run(self, t0: float, dt: float, nsteps: int):
+        self._rc(self.lib.ov_batch_run(self.h, t0, dt, nsteps))
+
+    def download(self, what: int = OV_FIELD_ALL):
+        self._rc(self.lib.ov_batch_download(self.h, self.t.ptr(), what))
+
+    def tuning(self) -> "_lib.BatchTuning":
+        tu = _lib.BatchTuning()
+        self._rc(self.lib.ov_batch_get_tuning(self.h, C.byref(tu)))
+        return tu
+
+    def set_tuning(self, targets_per_block: int, sources_per_tile: int, blocks_per_sm: int = 0):
+        tu = _lib.BatchTuning(targets_per_block, sources_per_tile, blocks_per_sm, 0.0)
+        self._rc(self.lib.ov_batch_set_tuning(self.h, C.byref(tu)))
+
+    def autotune(self) -> "_lib.BatchTuning":
+        tu = _lib.BatchTuning()
+        self._rc(self.lib.ov_batch_autotune(self.h, C.byref(tu)))
+        return tu
+
+    def stats(self) -> "_lib.BatchStats":
+        s = _lib.BatchStats()
+        self._rc(self.lib.ov_batch_get_stats(self.h, C.byref(s)))
+        return s
+
+    def close(self):
+        if self.h:
+            self.lib.ov_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -30,6 +30,9 @@ FUNCTIONS = [
     "ov_state_update_tangle", "ov_state_rk4_step", "ov_state_run", "ov_state_eval_points",
     "ov_measure_fma_peak", "ov_state_get_stats", "ov_state_reset_stats",
     "ov_set_mixed_near_factor", "ov_get_mixed_near_factor", "ov_direct_points_noalloc",
+    "ov_batch_create", "ov_batch_destroy", "ov_batch_update", "ov_batch_run",
+    "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
+    "ov_batch_get_stats",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -58,6 +61,17 @@ class RunStats(C.Structure):
                                           "bs_kernel_ms", "bs_launches", "build_ms",
                                           "last_run_ms", "launches", "n_targets", "n_segments",
                                           "warp_iterations")]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("targets_per_block", C.c_int), ("sources_per_tile", C.c_int),
+                ("blocks_per_sm", C.c_int), ("kernel_ms", C.c_double)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("evals", "interactions", "last_run_ms", "bs_kernel_ms",
+                                          "kernels_per_step", "n_targets", "n_segments",
+                                          "n_systems")]
 
 
 _lib = None
@@ -113,6 +127,15 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_get_mixed_near_factor": (C.c_double, []),
         "ov_direct_points_noalloc": (C.c_int, [T, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                                C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ov_batch_create": (C.c_void_p, [T, C.c_int, C.c_void_p]),
+        "ov_batch_destroy": (None, [C.c_void_p]),
+        "ov_batch_update": (C.c_int, [C.c_void_p, C.c_double]),
+        "ov_batch_run": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_int]),
+        "ov_batch_download": (C.c_int, [C.c_void_p, T, C.c_int]),
+        "ov_batch_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+        "ov_batch_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+        "ov_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
+        "ov_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -373,6 +373,10 @@ bool ov_capture_header_params(const struct tangle_state* t, OvParams& P) {
   return capture_params(t, P, false);
 }
 
+// Box, image table, globals and flows of a tangle (the pinned-node scan of
+// the boundary flow covers the tangle's N slots).
+bool ov_capture_params(const tangle_state* t, OvParams& P) { return capture_params(t, P, true); }
+
 // ======================================================================
 // state management
 
@@ -479,6 +483,27 @@ static bool sync(ov_state_impl* s) {
   return true;
 }
 
+bool ov_ensure_init() { return ensure_init(); }
+
+bool ov_upload_tangle(ov_state_impl* s, const tangle_state* t) { return upload_tangle(s, t, true); }
+
+bool ov_download_fields(ov_state_impl* s, tangle_state* t, int what) {
+  if (t->N != s->n) {
+    ov_set_error(OV_ERR_INVALID, "tangle has %d slots, state %d", t->N, s->n);
+    return false;
+  }
+  size_t n = (size_t)s->n;
+  if (n == 0) return true;
+  bool ok = true;
+  if (what & OV_FIELD_POS) ok = ok && download(s, t->vnodes, s->pos, 24 * n);
+  if (what & OV_FIELD_VELS) ok = ok && download(s, t->vels, s->vels, 24 * n);
+  if (what & OV_FIELD_VS) ok = ok && download(s, t->vs, s->vs, 24 * n);
+  if (what & OV_FIELD_TANGENTS) ok = ok && download(s, t->tangents, s->tan, 24 * n);
+  if (what & OV_FIELD_NORMALS) ok = ok && download(s, t->normals, s->nrm, 24 * n);
+  if (what & OV_FIELD_DXI) ok = ok && download(s, t->dxi, s->dxi, 8 * n);
+  return ok && sync(s);
+}
+
 bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* dxi,
                    const double* tan, const double* nrm, double* vels, double* vs,
                    OvTree* external_tree) {
@@ -558,18 +583,7 @@ int ov_state_upload(ov_state* st, const struct tangle_state* t) {
 int ov_state_download(ov_state* st, struct tangle_state* t, int what) {
   ov_clear_error();
   if (!st || !t) { ov_set_error(OV_ERR_INVALID, "null state or tangle"); return tl_err; }
-  ov_state_impl* s = &st->impl;
-  if (t->N != s->n) { ov_set_error(OV_ERR_INVALID, "tangle has %d slots, state %d", t->N, s->n); return tl_err; }
-  size_t n = (size_t)s->n;
-  if (n == 0) return OV_OK;
-  bool ok = true;
-  if (what & OV_FIELD_POS) ok = ok && download(s, t->vnodes, s->pos, 24 * n);
-  if (what & OV_FIELD_VELS) ok = ok && download(s, t->vels, s->vels, 24 * n);
-  if (what & OV_FIELD_VS) ok = ok && download(s, t->vs, s->vs, 24 * n);
-  if (what & OV_FIELD_TANGENTS) ok = ok && download(s, t->tangents, s->tan, 24 * n);
-  if (what & OV_FIELD_NORMALS) ok = ok && download(s, t->normals, s->nrm, 24 * n);
-  if (what & OV_FIELD_DXI) ok = ok && download(s, t->dxi, s->dxi, 8 * n);
-  if (!ok || !sync(s)) return tl_err;
+  if (!ov_download_fields(&st->impl, t, what)) return tl_err;
   return OV_OK;
 }
 
@@ -689,6 +703,9 @@ int ov_get_last_stats(ov_eval_stats* out) {
     float a = 0, b = 0;
     if (cudaEventElapsedTime(&a, s->ev0, s->ev1) == cudaSuccess) out->build_ms = a;
     if (cudaEventElapsedTime(&b, s->ev1, s->ev2) == cudaSuccess) out->eval_ms = b;
+    // an event not recorded yet fails the query above; drop that error so
+    // it is not reported by the next launch check
+    (void)cudaGetLastError();
     out->total_ms = out->build_ms + out->eval_ms;
   }
   return OV_OK;

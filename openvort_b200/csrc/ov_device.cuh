@@ -155,8 +155,12 @@ __device__ __forceinline__ d3 seg_vel64(double f4pi, d3 r1, d3 r2, d3 r) {
 // cut-off |cos - 1| < 1e-8 (src/tangle.c:505-506) zeroes far segments that
 // point within ~1e-4 rad of the target, so it is applied here too, through
 // 1 - cos = |R x ds|^2 / (|R||R'| (|R||R'| + R.R')), which has no
-// cancellation.  Returns false when the test is within 2e-5 (relative) of
-// the threshold: the caller then evaluates the segment in FP64.
+// cancellation.  Returns false when the test is within 2.5e-3 (relative) of
+// the threshold: the caller then evaluates the segment in FP64.  That band
+// bounds the FP32 error of |R x ds|^2: R and ds rounded once (2^-24 each)
+// and the cross product's own rounding give |dC| <= ~5e-7 |R||ds|, while
+// at the threshold |C| ~ 1.41e-4 |R|^2, so the relative error of C^2 is at
+// most ~7e-3 |ds|/|R| <= 1.8e-3 for |R| >= 4|ds|.
 __device__ __forceinline__ bool seg_vel32(float f4pi, float Rx, float Ry, float Rz,
                                           float dx, float dy, float dz,
                                           float& vx, float& vy, float& vz) {
@@ -171,8 +175,8 @@ __device__ __forceinline__ bool seg_vel32(float f4pi, float Rx, float Ry, float 
   float C2 = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
   float den = ab * (ab + RQ);
   vx = vy = vz = 0.f;
-  if (C2 < (1e-8f * (1.0f - 2e-5f)) * den) return true;   // colinear: zero
-  if (C2 <= (1e-8f * (1.0f + 2e-5f)) * den) return false; // too close to call
+  if (C2 < (1e-8f * (1.0f - 2.5e-3f)) * den) return true;   // colinear: zero
+  if (C2 <= (1e-8f * (1.0f + 2.5e-3f)) * den) return false; // too close to call
   // f (a+b) / (ab (ab + R.R'))
   float s = f4pi * (a + b) * ia * ib * __frcp_rn(ab + RQ);
   vx = cx * s; vy = cy * s; vz = cz * s;

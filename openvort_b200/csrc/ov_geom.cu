@@ -178,12 +178,15 @@ __global__ void k_tangents(OvParams P, Links L, const double* __restrict__ pos,
 }
 
 // velocity assembly per node (update_velocity, src/tangle.c:583-684)
-__global__ void k_epilogue(OvParams P, Links L, double t, const double* __restrict__ pos,
-                           const double* __restrict__ tan, const double* __restrict__ nrm,
-                           const double* __restrict__ v_nl, const double* __restrict__ v_img,
-                           double* vels, double* vs_out, int k0, int k1, int* flag) {
+// time = t0 + (*t_dev when given: a graph replayed at advancing times)
+__global__ void k_epilogue(OvParams P, Links L, const double* __restrict__ t_dev, double t0,
+                           const double* __restrict__ pos, const double* __restrict__ tan,
+                           const double* __restrict__ nrm, const double* __restrict__ v_nl,
+                           const double* __restrict__ v_img, double* vels, double* vs_out, int k0,
+                           int k1, int* flag) {
   int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= k1) return;
+  const double t = t_dev ? t0 + *t_dev : t0;
   int2 st = L.st[k];
   if (st.x == OV_EMPTY) return;
   d3 r = ld3(pos, k);
@@ -256,10 +259,56 @@ int blocks_for(int n) { return (n + kThreads - 1) / kThreads; }
 
 }  // namespace
 
-static bool check_flag(ov_state_impl* s, const char* where) {
-  int h = 0;
-  OV_TRY_CUDA(cudaMemcpyAsync(&h, s->dflag.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+// ---------------------------------------------------------------- launchers
+// Kernel launches only (no host synchronisation, so they can be captured in
+// a CUDA graph); link and finiteness errors accumulate in *flag.
+
+bool ov_launch_geometry(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                        const double* pos, double* dxi, double* tan, double* nrm, int n, int* flag) {
+  if (n <= 0) return true;
+  Links L{links, status};
+  k_dxi<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, n, flag);
+  OV_LAUNCHED();
+  k_tangents<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, tan, nrm, n, 0, flag);
+  OV_LAUNCHED();
+  k_tangents<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, tan, nrm, n, 1, flag);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_launch_epilogue(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                        const double* t_dev, double t0, const double* pos, const double* tan,
+                        const double* nrm, const double* v_nl, const double* v_img, double* vels,
+                        double* vs, int k0, int k1, int* flag) {
+  if (k1 <= k0) return true;
+  Links L{links, status};
+  k_epilogue<<<blocks_for(k1 - k0), kThreads, 0, st>>>(P, L, t_dev, t0, pos, tan, nrm, v_nl, v_img,
+                                                         vels, vs, k0, k1, flag);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_launch_euler(cudaStream_t st, const int2* status, const double* x0, const double* v,
+                     double h, double* xs, int n) {
+  if (n <= 0) return true;
+  k_euler<<<blocks_for(n), kThreads, 0, st>>>(status, x0, v, h, xs, n);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_launch_rk4_combine(cudaStream_t st, const int2* status, const double* k1, const double* k2,
+                           const double* k3, const double* k4, double dt, double* x, int n) {
+  if (n <= 0) return true;
+  k_rk4_combine<<<blocks_for(n), kThreads, 0, st>>>(status, k1, k2, k3, k4, dt, x, n);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_flag_status(int h, const char* where) {
   if (h & 1) {
     ov_set_error(OV_ERR_INVALID, "%s: broken vortex links (a free node without a neighbour)", where);
     return false;
@@ -271,18 +320,20 @@ static bool check_flag(ov_state_impl* s, const char* where) {
   return true;
 }
 
+static bool check_flag(ov_state_impl* s, const char* where) {
+  int h = 0;
+  OV_TRY_CUDA(cudaMemcpyAsync(&h, s->dflag.p, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return ov_flag_status(h, where);
+}
+
 bool ov_geometry(ov_state_impl* s, const double* pos, double* dxi, double* tan, double* nrm) {
   if (s->n == 0) return true;
-  Links L{s->links.as<int2>(), s->status.as<int2>()};
   int* flag = s->dflag.as<int>();
   OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
-  k_dxi<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->P, L, pos, dxi, s->n, flag);
-  OV_LAUNCHED();
-  k_tangents<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->P, L, pos, dxi, tan, nrm, s->n, 0, flag);
-  OV_LAUNCHED();
-  k_tangents<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->P, L, pos, dxi, tan, nrm, s->n, 1, flag);
-  OV_LAUNCHED();
-  OV_TRY_CUDA(cudaGetLastError());
+  if (!ov_launch_geometry(s->stream, s->P, s->links.as<int2>(), s->status.as<int2>(), pos, dxi, tan,
+                          nrm, s->n, flag))
+    return false;
   return check_flag(s, "update_tangents_normals");
 }
 
@@ -290,13 +341,11 @@ bool ov_epilogue(ov_state_impl* s, double t, const double* pos, const double* ta
                  const double* nrm, const double* v_nl, const double* v_img, double* vels,
                  double* vs, int k0, int k1) {
   if (k1 <= k0) return true;
-  Links L{s->links.as<int2>(), s->status.as<int2>()};
   int* flag = s->dflag.as<int>();
   OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
-  k_epilogue<<<blocks_for(k1 - k0), kThreads, 0, s->stream>>>(s->P, L, t, pos, tan, nrm, v_nl, v_img,
-                                                              vels, vs, k0, k1, flag);
-  OV_LAUNCHED();
-  OV_TRY_CUDA(cudaGetLastError());
+  if (!ov_launch_epilogue(s->stream, s->P, s->links.as<int2>(), s->status.as<int2>(), nullptr, t, pos,
+                          tan, nrm, v_nl, v_img, vels, vs, k0, k1, flag))
+    return false;
   return check_flag(s, "update_velocities");
 }
 

@@ -169,6 +169,29 @@ bool ov_epilogue(ov_state_impl* s, double t, const double* pos, const double* ta
 
 bool ov_state_reserve(ov_state_impl* s, int n);
 
+// Launches only, no host synchronisation (CUDA-graph capturable); link and
+// finiteness errors accumulate in *flag (bit 0 broken links, bit 1
+// non-finite velocity), read back later with ov_flag_status.
+bool ov_launch_geometry(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                        const double* pos, double* dxi, double* tan, double* nrm, int n, int* flag);
+// epilogue at time t0 + *t_dev (t_dev may be null: time t0)
+bool ov_launch_epilogue(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                        const double* t_dev, double t0, const double* pos, const double* tan,
+                        const double* nrm, const double* v_nl, const double* v_img, double* vels,
+                        double* vs, int k0, int k1, int* flag);
+bool ov_launch_euler(cudaStream_t st, const int2* status, const double* x0, const double* v,
+                     double h, double* xs, int n);
+bool ov_launch_rk4_combine(cudaStream_t st, const int2* status, const double* k1, const double* k2,
+                           const double* k3, const double* k4, double dt, double* x, int n);
+// error for flag bits h (false and the error set when any bit is set)
+bool ov_flag_status(int h, const char* where);
+
+// device selection on first use; the tangle's structure, positions and
+// parameters (globals, flows) into s; fields of s back into the tangle
+bool ov_ensure_init();
+bool ov_upload_tangle(ov_state_impl* s, const tangle_state* t);
+bool ov_download_fields(ov_state_impl* s, tangle_state* t, int what);
+
 // per-thread statistics of the last evaluation
 struct OvStatsAcc {
   double interactions, cell_interactions, cells, eval_ms, build_ms, total_ms, warp_iterations;

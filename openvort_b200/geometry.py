@@ -109,6 +109,26 @@ def ring_pair_system(rng: np.random.Generator, kind: str, n_total: int,
     return [a, b]
 
 
+def ring_pair_ensemble(seed: int, n_systems: int, n_range=(64, 2048), r_range=(5e-3, 2e-2),
+                       alloc=np.empty) -> Tuple[HostTangle, np.ndarray, List[List[np.ndarray]]]:
+    """Independent open-boundary systems for the batched path: each a coaxial
+    ring pair, leapfrogging or head-on (chosen at random), radii uniform in
+    r_range, total points uniform in n_range.  Returns the concatenated
+    tangle, the n_systems + 1 slot offsets, and each system's rings."""
+    rng = np.random.default_rng(seed)
+    systems = []
+    for _ in range(n_systems):
+        kind = "leapfrog" if rng.uniform() < 0.5 else "headon"
+        n_total = int(rng.integers(n_range[0], n_range[1] + 1))
+        systems.append(ring_pair_system(rng, kind, n_total, r_range))
+    rings = [r for sys_ in systems for r in sys_]
+    half = 2.0 * r_range[1] + 0.05
+    t = rings_to_tangle(rings, (-half,) * 3, (half,) * 3, "open", alloc=alloc)
+    sizes = [sum(len(r) for r in sys_) for sys_ in systems]
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    return t, offsets, systems
+
+
 def kelvin_ring(seed: int, n: int = 4096, radius: float = 1e-2, modes=(2, 32),
                 sigma: float = 1e-4) -> np.ndarray:
     """A ring with a seeded Kelvin-wave perturbation: radial and axial
