@@ -56,7 +56,10 @@ def _hbm_peak():
 
 HBM_PEAK, HBM_PEAK_SOURCE = _hbm_peak()
 FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
-WALK_DRAM_BYTES_PER_POINT = None  # dram__bytes_read.sum + dram__bytes_write.sum / points, ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of one mixed walk launch per
+# point, from the ncu launch list of this benchmark at 998,438 points
+# (323.1 MB per launch)
+WALK_DRAM_BYTES_PER_POINT = 323.6
 
 
 def parse():
