@@ -61,32 +61,32 @@ __device__ __forceinline__ double mac_dist2(const OvParams& P, d3 r, double cx, 
 // The reference's expansion (src/octree.c:303-328), moments pre-scaled by
 // kappa/4pi: gam x R / |R|^3 + (M21, 0, 0) / |R|^3 + (M.2 R_z) x R / |R|^5,
 // where (M.2 R_z) = (M02 Rz, M12 Rz, M22 Rz) is what its mat3_vmul returns.
+// Since (M.2 R_z) x R / |R|^5 = ((M.2) R_z / |R|^2) x R / |R|^3, the sum is
+// ((gam + M.2 R_z / |R|^2) x R + (M21, 0, 0)) / |R|^3: one cross product.
+// m = (M21, M02, M12, M22).
 __device__ __forceinline__ d3 expansion64(const double* g, const double* m, d3 R) {
-  double R2 = dot3(R, R);
-  double inv = 1.0 / sqrt(R2);
-  double i3 = inv * inv * inv;
-  double i5 = i3 * inv * inv;
-  d3 v = cross3(mk3(g[0], g[1], g[2]), R) * i3;
-  v.x += m[0] * i3;
-  d3 mv = mk3(m[1] * R.z, m[2] * R.z, m[3] * R.z);
-  return v + cross3(mv, R) * i5;
+  const double R2 = dot3(R, R);
+  const double inv = rsqrt(R2);
+  const double inv2 = inv * inv;
+  const double i3 = inv2 * inv;
+  const double w = R.z * inv2;
+  const d3 G = mk3(fma(m[1], w, g[0]), fma(m[2], w, g[1]), fma(m[3], w, g[2]));
+  const d3 c = cross3(G, R);
+  return mk3((c.x + m[0]) * i3, c.y * i3, c.z * i3);
 }
 
 __device__ __forceinline__ void expansion32(float g0, float g1, float g2, float m21, float m02,
                                             float m12, float m22, float Rx, float Ry, float Rz,
                                             float& vx, float& vy, float& vz) {
-  float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
-  float inv = rsqrtf(R2);
-  float i3 = inv * inv * inv;
-  float i5 = i3 * inv * inv;
-  float cx = g1 * Rz - g2 * Ry;
-  float cy = g2 * Rx - g0 * Rz;
-  float cz = g0 * Ry - g1 * Rx;
-  float ax = m02 * Rz, ay = m12 * Rz, az = m22 * Rz;
-  float qx = ay * Rz - az * Ry, qy = az * Rx - ax * Rz, qz = ax * Ry - ay * Rx;
-  vx = fmaf(cx + m21, i3, qx * i5);
-  vy = fmaf(cy, i3, qy * i5);
-  vz = fmaf(cz, i3, qz * i5);
+  const float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
+  const float inv = rsqrtf(R2);
+  const float inv2 = inv * inv;
+  const float i3 = inv2 * inv;
+  const float w = Rz * inv2;
+  const float Gx = fmaf(m02, w, g0), Gy = fmaf(m12, w, g1), Gz = fmaf(m22, w, g2);
+  vx = fmaf(Gy, Rz, fmaf(-Gz, Ry, m21)) * i3;
+  vy = fmaf(Gz, Rx, -Gx * Rz) * i3;
+  vz = fmaf(Gx, Ry, -Gy * Rx) * i3;
 }
 
 __device__ __forceinline__ void prefetch_l1(const void* p) {
@@ -255,6 +255,32 @@ __device__ __forceinline__ double img_coord(double r, double L, int i) {
   return i == 1 ? r : (i == 0 ? __dsub_rn(r, -L) : __dsub_rn(r, L));
 }
 
+// The 27 opening decisions of a cell (wrapped squared distance of each
+// image point to the centre of mass >= thr), exactly with the reference's
+// FP64 operations: per axis and shift the wrapped square, summed x + y then
+// + z as segment_len does (src/octree.c:284-296).  All 27 are independent.
+__device__ __forceinline__ unsigned mac_exact(const OvParams& P, d3 r, double cx, double cy,
+                                              double cz, double thr) {
+  const double qx[3] = {wrapped_sq(P, 0, img_coord(r.x, P.L[0], 0), cx), wrapped_sq(P, 0, r.x, cx),
+                        wrapped_sq(P, 0, img_coord(r.x, P.L[0], 2), cx)};
+  const double qy[3] = {wrapped_sq(P, 1, img_coord(r.y, P.L[1], 0), cy), wrapped_sq(P, 1, r.y, cy),
+                        wrapped_sq(P, 1, img_coord(r.y, P.L[1], 2), cy)};
+  const double qz[3] = {wrapped_sq(P, 2, img_coord(r.z, P.L[2], 0), cz), wrapped_sq(P, 2, r.z, cz),
+                        wrapped_sq(P, 2, img_coord(r.z, P.L[2], 2), cz)};
+  unsigned pass = 0;
+#pragma unroll
+  for (int ix = 0; ix < 3; ++ix) {
+#pragma unroll
+    for (int iy = 0; iy < 3; ++iy) {
+      const double qxy = __dadd_rn(qx[ix], qy[iy]);
+#pragma unroll
+      for (int iz = 0; iz < 3; ++iz)
+        pass |= (__dadd_rn(qxy, qz[iz]) >= thr ? 1u : 0u) << (9 * ix + 3 * iy + iz);
+    }
+  }
+  return pass;
+}
+
 template <bool kMixed>
 __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 r, d3 r1, d3 r2,
                                            int id, int fw, int skip, double near2, d3& nl, d3& im,
@@ -281,20 +307,34 @@ __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 
       float vx, vy, vz;
       if (R2 >= far2 && ds2 > 0 &&
           seg_vel32(f4, (float)R.x, (float)R.y, (float)R.z, dsx, dsy, dsz, vx, vy, vz)) {
-        if (c == kPrimary) nl = nl + mk3(vx, vy, vz);
-        else { fx += vx; fy += vy; fz += vz; }
+        fx += vx; fy += vy; fz += vz;
         continue;
       }
+      // the mixed form keeps one sum for the tangle and its images
+      nl = nl + seg64_at(P.f4pi, r1, r2, t);
+      continue;
     }
     const d3 v = seg64_at(P.f4pi, r1, r2, t);
     if (c == kPrimary) nl = nl + v;
     else im = im + v;
   }
-  if (kMixed) im = im + mk3(fx, fy, fz);
+  if (kMixed) nl = nl + mk3(fx, fy, fz);
 }
 
+// resident blocks per SM the register allocation must allow (measured at
+// 1M points: the walk is latency-bound, so more resident warps pay even
+// with a few registers spilled to L1)
+#ifndef OV_WALK_MULTI_MIN_BLOCKS_MIXED
+#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 6
+#endif
+#ifndef OV_WALK_MULTI_MIN_BLOCKS_FP64
+#define OV_WALK_MULTI_MIN_BLOCKS_FP64 5
+#endif
+
 template <bool kMixed>
-__global__ void __launch_bounds__(kMultiWarps * 32) k_walk_multi(
+__global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_BLOCKS_MIXED
+                                                           : OV_WALK_MULTI_MIN_BLOCKS_FP64)
+    k_walk_multi(
     OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
     const double* __restrict__ pos, int n_t, unsigned combos, double near2, double* v_nl,
     double* v_img, unsigned long long* counters) {
@@ -333,25 +373,18 @@ __global__ void __launch_bounds__(kMultiWarps * 32) k_walk_multi(
       } else if (kind == CELL_LEAFN) {
         p2p_mask = m;
       } else {
-        // opening test per image (octree_get_vs, src/octree.c:284-296): the
-        // wrapped squared distance, summed x + y then + z as the reference does
+        // opening test per image (octree_get_vs, src/octree.c:284-296)
         const double cx = t0.y, cy = t1.x, cz = t1.y;
-        const double qx[3] = {wrapped_sq(P, 0, img_coord(r.x, P.L[0], 0), cx), wrapped_sq(P, 0, r.x, cx),
-                              wrapped_sq(P, 0, img_coord(r.x, P.L[0], 2), cx)};
-        const double qy[3] = {wrapped_sq(P, 1, img_coord(r.y, P.L[1], 0), cy), wrapped_sq(P, 1, r.y, cy),
-                              wrapped_sq(P, 1, img_coord(r.y, P.L[1], 2), cy)};
-        const double qz[3] = {wrapped_sq(P, 2, img_coord(r.z, P.L[2], 0), cz), wrapped_sq(P, 2, r.z, cz),
-                              wrapped_sq(P, 2, img_coord(r.z, P.L[2], 2), cz)};
-        unsigned pass = 0;
-#pragma unroll 1
-        for (int xy = 0; xy < 9; ++xy) {
-          if (!(m & (7u << (3 * xy)))) continue;
-          const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
-          const double qxy = __dadd_rn(sel3(ix, qx[0], qx[1], qx[2]), sel3(iy, qy[0], qy[1], qy[2]));
-#pragma unroll
-          for (int iz = 0; iz < 3; ++iz)
-            if (__dadd_rn(qxy, qz[iz]) >= t0.x) pass |= 1u << (3 * xy + iz);
-        }
+        // Every image point is at least as far from the centre of mass as the
+        // target itself, per axis, in exact arithmetic.  The FP64 rounding of
+        // a wrapped square is at most ~2e-16 L per component, i.e. below
+        // 1e-11 of thr for the smallest cells, so when the target passes with
+        // a 1e-10 margin every image passes too.  Otherwise all 27 decisions.
+        unsigned pass;
+        const double q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)),
+                                    wrapped_sq(P, 2, r.z, cz));
+        if (q0 >= t0.x * (1.0 + 1e-10)) pass = m;
+        else pass = mac_exact(P, r, cx, cy, cz, t0.x);
         pass &= m;
         const unsigned fail = m & ~pass;
         if (kind == CELL_OPEN) open = fail;
@@ -363,17 +396,21 @@ __global__ void __launch_bounds__(kMultiWarps * 32) k_walk_multi(
             const float2 f0 = *reinterpret_cast<const float2*>(&cp->f_g[0]);
             const float2 f1 = *reinterpret_cast<const float2*>(&cp->f_g[2]);
             const float2 f2 = *reinterpret_cast<const float2*>(&cp->f_m12);
+            const float g0 = f0.x, g1 = f0.y, g2 = f1.x, m02 = f1.y, m12 = f2.x, m22 = f2.y;
             const float m21 = __int_as_float(h.x);
-            // FP32 copies of the FP64-formed offsets per axis and shift
-            const float Fx0 = (float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
-                        Fx1 = (float)__dsub_rn(r.x, cx),
-                        Fx2 = (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx);
-            const float Fy0 = (float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
-                        Fy1 = (float)__dsub_rn(r.y, cy),
-                        Fy2 = (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy);
+            // FP32 copies of the FP64-formed offsets r - L s - com per axis and shift
+            const float Fx[3] = {(float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
+                                 (float)__dsub_rn(r.x, cx),
+                                 (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx)};
+            const float Fy[3] = {(float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
+                                 (float)__dsub_rn(r.y, cy),
+                                 (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy)};
             const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
                                  (float)__dsub_rn(r.z, cz),
                                  (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+            // an accepting image has |R|^2 >= its wrapped squared distance >=
+            // thr, so a cell whose thr reaches the near radius needs no test
+            const bool test_near = t0.x < near2;
             const float fnear2 = (float)near2;
             float ax = 0, ay = 0, az = 0;
 #pragma unroll 1
@@ -381,28 +418,43 @@ __global__ void __launch_bounds__(kMultiWarps * 32) k_walk_multi(
               const unsigned bits = (pass >> (3 * xy)) & 7u;
               if (!bits) continue;
               const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
-              const float X = sel3f(ix, Fx0, Fx1, Fx2);
-              const float Y = sel3f(iy, Fy0, Fy1, Fy2);
+              const float X = sel3f(ix, Fx[0], Fx[1], Fx[2]);
+              const float Y = sel3f(iy, Fy[0], Fy[1], Fy[2]);
+              const float XY2 = fmaf(X, X, Y * Y);
+              // no z image of the column is nearer than its (x, y) distance
+              const bool col_near = test_near && XY2 < fnear2;
+              // the column's three z images evaluated side by side (independent
+              // chains), summed where they accept the cell
 #pragma unroll
               for (int iz = 0; iz < 3; ++iz) {
-                if (!((bits >> iz) & 1u)) continue;
-                const int c = 3 * xy + iz;
                 const float Z = Fz[iz];
-                if (fmaf(X, X, fmaf(Y, Y, Z * Z)) < fnear2) {
+                const float R2 = fmaf(Z, Z, XY2);
+                const float inv = rsqrtf(R2);
+                const float inv2 = inv * inv;
+                const float i3 = inv2 * inv;
+                const float w = Z * inv2;
+                const float Gx = fmaf(m02, w, g0), Gy = fmaf(m12, w, g1), Gz = fmaf(m22, w, g2);
+                const float cxv = fmaf(Gy, Z, fmaf(-Gz, Y, m21));
+                const float cyv = fmaf(Gz, X, -Gx * Z);
+                const float czv = fmaf(Gx, Y, -Gy * X);
+                bool on = (bits >> iz) & 1u;
+                if (on && col_near && R2 < fnear2) {
                   // near field: FP64 expansion from the FP64 offsets
                   const d3 v = expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ix), cx),
                                                       __dsub_rn(img_coord(r.y, P.L[1], iy), cy),
                                                       __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
-                  if (c == kPrimary) nl = nl + v; else im = im + v;
-                  continue;
+                  nl = nl + v;
+                  on = false;
                 }
-                float vx, vy, vz;
-                expansion32(f0.x, f0.y, f1.x, m21, f1.y, f2.x, f2.y, X, Y, Z, vx, vy, vz);
-                if (c == kPrimary) nl = nl + mk3(vx, vy, vz);
-                else { ax += vx; ay += vy; az += vz; }
+                if (on) {
+                  ax = fmaf(cxv, i3, ax);
+                  ay = fmaf(cyv, i3, ay);
+                  az = fmaf(czv, i3, az);
+                }
               }
             }
-            im = im + mk3(ax, ay, az);
+            // the mixed form keeps one sum for the tangle and its images
+            nl = nl + mk3(ax, ay, az);
           } else {
             const double g[3] = {cp->y[0], cp->y[1], cp->y[2]};
             const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
