@@ -75,6 +75,8 @@ def parse():
     ap.add_argument("--fp64-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the direct-sum and batch lines")
+    ap.add_argument("--batch-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -248,6 +250,98 @@ def run_reference_arm(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU side
+def bench_direct(args, ov, peak32: float, peak64: float):
+    """Direct all-pairs kernel on the 22.4k-point periodic tangle: 512 rings
+    in a periodic cube D = 0.1 cm, radii U[0.02, 0.05] D, dl = D/200, 26
+    images.  Kernel time per evaluation (CUDA events around the kernel)
+    against 43 flops per segment-point interaction, mixed and FP64."""
+    from openvort_b200 import geometry as G
+    from openvort_b200.tangle import Flow, Params
+    D2 = 0.1
+    dl2 = D2 / 200
+    t = G.random_ring_tangle(args.seed + 2, 512, D2, dl=dl2, boundary="periodic-26")
+    p = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=2 * dl2, hyperfriction=1,
+               use_bh=0, vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}), vs=Flow("no flow"))
+    out = {"workload": f"512 rings, {int(t.active.sum())} points, periodic cube D=0.1 cm, 26 images, "
+                       f"direct sum", "points": int(t.active.sum())}
+    vel = {}
+    for name, prec, peak in (("mixed", ov.OV_PREC_MIXED, peak32), ("fp64", ov.OV_PREC_FP64, peak64)):
+        ov.configure(p, prec)
+        st = ov.DeviceState(t.copy())
+        st.update_tangle(0.0)
+        st.reset_stats()
+        for _ in range(5):
+            st.update_tangle(0.0)
+        rs = st.stats()
+        ms = rs.bs_kernel_ms / rs.bs_launches
+        inter = rs.interactions / rs.bs_launches
+        tf = inter * FLOPS_P2P / (ms / 1e3) / 1e12
+        out[name] = {"kernel_ms": ms, "interactions": inter, "tflops": tf, "peak_tflops": peak,
+                     "frac": tf / peak if peak else None,
+                     "point_evals_per_s": out["points"] / (ms / 1e3)}
+        st.download()
+        vel[name] = st.t.vels.copy()
+        st.close()
+    act = t.active
+    num = np.linalg.norm(vel["mixed"][act] - vel["fp64"][act], axis=1)
+    den = np.linalg.norm(vel["fp64"][act], axis=1)
+    out["max_rel_err_mixed_vs_fp64"] = float(np.max(num / den))
+    out["mixed_over_fp64_speedup"] = out["fp64"]["kernel_ms"] / out["mixed"]["kernel_ms"]
+    return out
+
+
+def bench_batch(args, ov, peak32: float):
+    """Batched ensemble: 4096 independent open-boundary ring pairs (leapfrog
+    or head-on), radii U[5e-3, 2e-2] cm, U[64, 2048] points per system, mixed
+    form, one persistent Biot-Savart kernel per RK4 stage, CUDA graph per
+    step, autotuned kernel shape."""
+    from openvort_b200 import geometry as G
+    from openvort_b200.tangle import Flow, Params
+    t, off, _ = G.ring_pair_ensemble(args.seed + 4, 4096, n_range=(64, 2048))
+    p = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=1e-2, hyperfriction=0,
+               use_bh=0, vn=Flow("no flow"), vs=Flow("no flow"))
+    # the finest systems (2048 points on r = 5e-3 cm rings, spacing 3e-5 cm)
+    # carry Kelvin waves of frequency ~5e6 /s at the grid scale: RK4 needs
+    # dt below ~5e-7 s there
+    dt = 2.5e-7
+    n = int(t.active.sum())
+    out = {"workload": f"4096 ring-pair systems, {n} points, open boundaries, direct sums per system, "
+                       f"RK4 dt={dt}", "points": n, "systems": 4096, "steps": args.batch_steps}
+    ov.configure(p, ov.OV_PREC_MIXED)
+    b = ov.DeviceBatch(t.copy(), off)
+    tu = b.autotune()
+    out["tuning"] = {"targets_per_block": tu.targets_per_block, "sources_per_tile": tu.sources_per_tile,
+                     "blocks_per_sm": tu.blocks_per_sm}
+    b.run(0.0, dt, 2)
+    b.run(2 * dt, dt, args.batch_steps)
+    st = b.stats()
+    ms_step = st.last_run_ms / args.batch_steps
+    inter = st.interactions / st.evals
+    tf = inter * FLOPS_P2P / (st.bs_kernel_ms / 1e3) / 1e12
+    out.update({"value": n * 4 / (ms_step / 1e3), "unit": UNIT, "ms_per_step": ms_step,
+                "rk4_steps_per_s": 1e3 / ms_step, "kernels_per_step": st.kernels_per_step,
+                "bs_kernel_ms": st.bs_kernel_ms, "interactions_per_eval": inter,
+                "roofline": {"bound": "fp32", "achieved": tf, "peak": peak32, "unit": "TFLOP/s",
+                             "frac": tf / peak32 if peak32 else None}})
+    b.close()
+    # FP64 form of the same ensemble: kernel time and the mixed error
+    vel = {}
+    for name, prec in (("fp64", ov.OV_PREC_FP64), ("mixed", ov.OV_PREC_MIXED)):
+        ov.configure(p, prec)
+        bb = ov.DeviceBatch(t.copy(), off)
+        bb.autotune()
+        bb.update(0.0)
+        bb.download()
+        vel[name] = bb.t.vels.copy()
+        if name == "fp64":
+            out["fp64_bs_kernel_ms"] = bb.stats().bs_kernel_ms
+        bb.close()
+    num = np.linalg.norm(vel["mixed"] - vel["fp64"], axis=1)
+    den = np.linalg.norm(vel["fp64"], axis=1)
+    out["max_rel_err_mixed_vs_fp64"] = float(np.max(num / den))
+    return out
+
+
 def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
@@ -382,6 +476,11 @@ def main():
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
 
+    direct = batch = None
+    if not args.no_extra:
+        direct = bench_direct(args, ov, peak32.value, peak64.value)
+        batch = bench_batch(args, ov, peak32.value)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_sample(tangle, p, target_s=10.0)
@@ -421,6 +520,8 @@ def main():
                                   "peak_source": HBM_PEAK_SOURCE + " copy bandwidth"}
                                  if traffic else None),
                          "tree_build_share_of_step": build_share},
+            "direct_22k": direct,
+            "batch_4096": batch,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -230,7 +230,8 @@ int ov_get_precision(void);
 void ov_set_rk4_classic(int classic);
 int ov_get_rk4_classic(void);
 /* Mixed form: interactions closer than factor * global_dl_max to the target
- * (segments and cell expansions) are evaluated in FP64 (default 16). */
+ * (segments and cell expansions) are evaluated in FP64 (default 8; segments
+ * nearer than 4 times their own length always are). */
 void ov_set_mixed_near_factor(double factor);
 double ov_get_mixed_near_factor(void);
 

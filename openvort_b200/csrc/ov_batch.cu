@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "ov_internal.h"
+#include "ov_pair.cuh"
 
 namespace {
 
@@ -87,11 +88,15 @@ __global__ void __launch_bounds__(TB) k_batch_bs64(OvParams P, BatchView B,
   }
 }
 
-// Mixed form: positions as two-float offsets (hi + lo) from the item's first
-// target, so R = (a_hi - t_hi) + (a_lo - t_lo) carries ~2 FP32 ulps of |R|;
-// segments beyond max(4 |ds|, the system's near radius) take the FP32
-// formula, the others the FP64 one from the FP64 positions; FP32 partial
-// sums over 32 sources are added into FP64 sums.
+// Mixed form: two-float FP32 offsets from the item's first target (the
+// systems' targets and sources span whole rings, so a single rounding of
+// the offsets would cost a near segment ~1e-6 of its |R|), two sources per
+// f32x2 instruction and kTT targets per thread (pair_interact); pairs
+// nearer than max(4 |ds|, the system's near radius) or too close to the
+// colinearity cut-off take the FP64 formula from the FP64 positions.  FP32
+// partial sums over 32 sources are added into FP64 sums.  With open
+// boundaries the two segments the skip rule drops have an endpoint at the
+// target, so they are near and the FP64 cut-off returns zero for them.
 template <int TB, int TS>
 __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
                                                        const double* __restrict__ pos,
@@ -99,12 +104,10 @@ __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
                                                        const int2* __restrict__ status,
                                                        double* __restrict__ v_nl,
                                                        int* __restrict__ work) {
-  __shared__ float4 sh_hi[TS];   // r1 - O (hi), w = squared FP32 radius
-  __shared__ float4 sh_lo[TS];   // r1 - O (lo)
-  __shared__ float4 sh_d[TS];    // ds
-  __shared__ int2 sh_id[TS];     // segment start and end slots (-1: none)
+  static_assert(TS % 32 == 0, "sources per tile");
+  __shared__ PairSrc<true> sh[TS / 2];
   __shared__ int sh_item;
-  const float f4 = (float)P.f4pi;
+  const double f4pi = P.f4pi;
   for (;;) {
     __syncthreads();
     if (threadIdx.x == 0) sh_item = atomicAdd(work, 1);
@@ -115,67 +118,68 @@ __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
     const int s0 = B.off[w.x], s1 = B.off[w.x + 1];
     const double near2 = B.near2[w.x];
     const d3 O = ld3(pos, w.y);
-    const int k = w.y + threadIdx.x;
-    const bool act = k < s1 && status[k].x == OV_FREE;
-    const d3 r = act ? ld3(pos, k) : O;
-    const double ex = r.x - O.x, ey = r.y - O.y, ez = r.z - O.z;
-    const float thx = (float)ex, thy = (float)ey, thz = (float)ez;
-    const float tlx = (float)(ex - thx), tly = (float)(ey - thy), tlz = (float)(ez - thz);
-    double ax = 0, ay = 0, az = 0;
+    int kk[kTT];
+    PairTargets T;
+    double acc[kTT][3];
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) {
+      const int k = w.y + threadIdx.x + TB * u;
+      const bool act = k < s1 && status[k].x == OV_FREE;
+      kk[u] = act ? k : -1;
+      const d3 r = act ? ld3(pos, k) : O;
+      set_target(T, u, r.x - O.x, r.y - O.y, r.z - O.z);
+      acc[u][0] = acc[u][1] = acc[u][2] = 0;
+    }
+    auto special = [&](int u, int id) {
+#pragma unroll
+      for (int v = 0; v < kTT; ++v) {
+        if (v != u) continue;
+        const int k = kk[v];
+        if (k < 0 || id < 0) return;
+        const d3 vv = seg_vel64(f4pi, ld3(pos, id), ld3(pos, links[id].x), ld3(pos, k));
+        acc[v][0] += vv.x;
+        acc[v][1] += vv.y;
+        acc[v][2] += vv.z;
+      }
+    };
+    auto stage_one = [&](int m) -> SrcVals {
+      if (m >= s1 || status[m].x == OV_EMPTY) return src_none();
+      const int f = links[m].x;
+      if (f < 0) return src_none();
+      const d3 a = ld3(pos, m), bb = ld3(pos, f);
+      const double dx = bb.x - a.x, dy = bb.y - a.y, dz = bb.z - a.z;
+      const double far2 = fmax(16.0 * (dx * dx + dy * dy + dz * dz), near2);
+      return src_from(a.x - O.x, a.y - O.y, a.z - O.z, dx, dy, dz, far2, m);
+    };
     for (int base = s0; base < s1; base += TS) {
       __syncthreads();
-      for (int q = threadIdx.x; q < TS; q += TB) {
-        const int m = base + q;
-        float4 hi = make_float4((float)kNoSeg, (float)kNoSeg, (float)kNoSeg, 0.f);
-        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), d = lo;
-        int2 id = make_int2(-1, -1);
-        if (m < s1 && status[m].x != OV_EMPTY) {
-          const int f = links[m].x;
-          if (f >= 0) {
-            const d3 a = ld3(pos, m), b = ld3(pos, f);
-            const double dx = b.x - a.x, dy = b.y - a.y, dz = b.z - a.z;
-            const double px = a.x - O.x, py = a.y - O.y, pz = a.z - O.z;
-            const float hx = (float)px, hy = (float)py, hz = (float)pz;
-            hi = make_float4(hx, hy, hz, (float)fmax(16.0 * (dx * dx + dy * dy + dz * dz), near2));
-            lo = make_float4((float)(px - hx), (float)(py - hy), (float)(pz - hz), 0.f);
-            d = make_float4((float)dx, (float)dy, (float)dz, 0.f);
-            id = make_int2(m, f);
-          }
-        }
-        sh_hi[q] = hi;
-        sh_lo[q] = lo;
-        sh_d[q] = d;
-        sh_id[q] = id;
-      }
+      for (int q = threadIdx.x; q < TS / 2; q += TB)
+        stage_pair(sh[q], stage_one(base + 2 * q), stage_one(base + 2 * q + 1));
       __syncthreads();
-      if (!act) continue;
-      const int cnt = min(TS, s1 - base);
-      for (int q0 = 0; q0 < cnt; q0 += 32) {
-        float bx = 0, by = 0, bz = 0;
-        const int q1 = min(q0 + 32, cnt);
-        for (int q = q0; q < q1; ++q) {
-          const float4 a = sh_hi[q];
-          const float4 l = sh_lo[q];
-          const float4 dd = sh_d[q];
-          const float Rx = (a.x - thx) + (l.x - tlx);
-          const float Ry = (a.y - thy) + (l.y - tly);
-          const float Rz = (a.z - thz) + (l.z - tlz);
-          const float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
-          float vx, vy, vz;
-          if (R2 >= a.w && seg_vel32(f4, Rx, Ry, Rz, dd.x, dd.y, dd.z, vx, vy, vz)) {
-            bx += vx; by += vy; bz += vz;
-          } else {
-            const int2 id = sh_id[q];
-            if (id.x >= 0) {
-              const d3 v = seg_vel64(P.f4pi, ld3(pos, id.x), ld3(pos, id.y), r);
-              ax += v.x; ay += v.y; az += v.z;
-            }
+      const int nrec = (min(TS, s1 - base) + 1) / 2;   // records holding a source
+      for (int q0 = 0; q0 < nrec; q0 += 16) {
+        f2 bsum[kTT][3];
+#pragma unroll
+        for (int k = 0; k < kTT; ++k) bsum[k][0] = bsum[k][1] = bsum[k][2] = f2_splat(0.f);
+        const int q1 = min(q0 + 16, nrec);
+#pragma unroll 2
+        for (int q = q0; q < q1; ++q) pair_interact<true>(sh[q], T, bsum, special);
+#pragma unroll
+        for (int k = 0; k < kTT; ++k) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            float lo, hi;
+            f2_unpack(bsum[k][c], lo, hi);
+            acc[k][c] += f4pi * ((double)lo + (double)hi);
           }
         }
-        ax += bx; ay += by; az += bz;
       }
     }
-    if (k < s1) st3(v_nl, k, act ? mk3(ax, ay, az) : mk3(0, 0, 0));
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) {
+      const int k = w.y + threadIdx.x + TB * u;
+      if (k < s1) st3(v_nl, k, kk[u] >= 0 ? mk3(acc[u][0], acc[u][1], acc[u][2]) : mk3(0, 0, 0));
+    }
   }
 }
 
@@ -301,12 +305,15 @@ int grid_for(const ov_batch* b, bool mixed) {
 
 // the Biot-Savart sum of every system at positions pos -> v_nl; work: a
 // zeroed counter
+// targets per work item of a kernel shape and form
+int item_targets(int shape, bool mixed) { return kShapes[shape].tb * (mixed ? kTT : 1); }
+
 bool launch_bs(ov_batch* b, const double* pos, double* v_nl, int* work) {
   const Shape& sh = kShapes[b->shape];
-  if (!build_items(b, sh.tb)) return false;
+  const bool mixed = b->s.P.precision == OV_PREC_MIXED;
+  if (!build_items(b, item_targets(b->shape, mixed))) return false;
   if (b->n_items == 0) return true;
   BatchView B{b->d_off.as<int>(), b->d_items.as<int2>(), b->d_near2.as<double>(), b->n_items};
-  const bool mixed = b->s.P.precision == OV_PREC_MIXED;
   BsKernel k = mixed ? sh.kmixed : sh.k64;
   if (!g_occ[b->shape][mixed ? 1 : 0] && !prepare_shape(b->shape, mixed)) return false;
   const int grid = grid_for(b, mixed);
@@ -561,7 +568,7 @@ int ov_batch_run(ov_batch* b, double t0, double dt, int nsteps) {
   // one RK4 step as a graph (the parameters, the kernel shape and dt are
   // baked in, so it is captured again on every call)
   drop_graph(b);
-  if (!build_items(b, kShapes[b->shape].tb) ||
+  if (!build_items(b, item_targets(b->shape, s->P.precision == OV_PREC_MIXED)) ||
       !prepare_shape(b->shape, s->P.precision == OV_PREC_MIXED))
     return ov_last_error();
   const long long before = ov_launches();

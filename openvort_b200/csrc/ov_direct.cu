@@ -10,11 +10,13 @@
 // summed in image-table order so the result is deterministic.
 //
 // FP64 form: the reference's formula and cut-offs (seg_vel64).
-// Mixed form: sources staged as FP32 offsets from the block's first target
-// (the subtraction done in FP64, rounded once); far segments (|R| >= 4|ds|)
-// take the FP32 formula, near ones fall back to seg_vel64 from the FP64
-// table; sums accumulate in FP64.
+// Mixed form (k_direct_mixed_pairs): sources staged two by two as FP32
+// offsets from the block's first target (the subtraction done in FP64,
+// rounded once) and evaluated two per f32x2 instruction (ov_pair.cuh); near
+// or borderline-colinear pairs fall back to seg_vel64 from the FP64 table;
+// sums accumulate in FP64.
 #include "ov_internal.h"
+#include "ov_pair.cuh"
 
 namespace {
 
@@ -98,105 +100,112 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
   }
 }
 
-// Mixed form.  Segments closer than max(4 |ds|, the near radius) use the
-// FP64 formula from the FP64 table.  Sources and targets are FP64 offsets from the block origin O
-// (the block's first target's point for this image) split into two FP32
-// parts, hi = fl32(p - O) and lo = fl32((p - O) - hi); R = (a_hi - t_hi) +
-// (a_lo - t_lo) then carries ~2 FP32 ulps of |R| itself, however far the
-// source and target are from O.
-__global__ void __launch_bounds__(kTB) k_direct_mixed(OvParams P, SegTab S, int n_src,
-                                                      const double* __restrict__ tpos,
-                                                      const int2* __restrict__ tstatus,
-                                                      const int* __restrict__ order, int n_t,
-                                                      int stride, double* __restrict__ part) {
-  __shared__ float4 sh_hi[kTS];   // r1 - O (hi part), w = 16 |ds|^2
-  __shared__ float4 sh_lo[kTS];   // r1 - O (lo part)
-  __shared__ float4 sh_d[kTS];    // ds
-  __shared__ int sh_id[kTS][2];
-  __shared__ double sh_O[3];
-  const int j = blockIdx.y;
-  const int i = blockIdx.x * kTB + threadIdx.x;   // position in `order`
-  int k = i < n_t ? (order ? order[i] : i) : -1;
-  bool act = k >= 0 && tstatus[k].x != OV_EMPTY && tstatus[k].x != OV_PINNED;
-  d3 r = mk3(0, 0, 0);
-  if (k >= 0) {
-    r = ld3(tpos, k);
-    if (j > 0) r = image_point(P, j - 1, r);
+// Mixed form, two sources per instruction.  Block = kPB threads x kTT
+// targets (the tree's key order, so close in space) x one image.  The
+// origin O is the block's first target, so a single rounding of the
+// offsets costs R a few FP32 ulps of |R| + (the block's extent).  A segment
+// wrapped across a periodic face may be the one the skip rule drops for its
+// end node; for the tangle itself (image 0) it is always evaluated in FP64,
+// where that rule is applied.
+//
+// Shape measured on the 22.4k-point periodic tangle: 128 threads of 2
+// targets, at most 96 registers (5 resident blocks per SM), two records per
+// unrolled step.
+constexpr int kPB = 128;            // threads per block
+constexpr int kPTgt = kPB * kTT;    // targets per block
+constexpr int kPSrc = 128;          // sources per shared-memory tile (kPSrc / 2 records)
+
+__global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
+    OvParams P, SegTab S, int n_src, const double* __restrict__ pos, const int2* __restrict__ tstatus,
+    const int* __restrict__ order, int n_t, int stride, double* __restrict__ part) {
+  __shared__ PairSrc<false> sh[kPSrc / 2];
+  const int j = blockIdx.y;   // 0: the tangle itself, j >= 1: image j-1
+  const int base = blockIdx.x * kPTgt;
+  d3 O = ld3(pos, order[base]);
+  if (j > 0) O = image_point(P, j - 1, O);
+  int kk[kTT];
+  PairTargets T;
+#pragma unroll
+  for (int u = 0; u < kTT; ++u) {
+    const int i = base + threadIdx.x + kPB * u;
+    int k = i < n_t ? order[i] : -1;
+    if (k >= 0 && (tstatus[k].x == OV_EMPTY || tstatus[k].x == OV_PINNED)) k = -1;
+    kk[u] = k;
+    d3 r = O;
+    if (k >= 0) {
+      r = ld3(pos, k);
+      if (j > 0) r = image_point(P, j - 1, r);
+    }
+    set_target(T, u, r.x - O.x, r.y - O.y, r.z - O.z);
   }
-  if (threadIdx.x == 0) {
-    int k0 = order ? order[blockIdx.x * kTB] : blockIdx.x * kTB;
-    d3 o = ld3(tpos, k0);
-    if (j > 0) o = image_point(P, j - 1, o);
-    sh_O[0] = o.x; sh_O[1] = o.y; sh_O[2] = o.z;
-  }
-  __syncthreads();
-  const d3 O = mk3(sh_O[0], sh_O[1], sh_O[2]);
-  const int skip = (j == 0) ? k : -1;
-  const double ex = r.x - O.x, ey = r.y - O.y, ez = r.z - O.z;
-  const float thx = (float)ex, thy = (float)ey, thz = (float)ez;
-  const float tlx = (float)(ex - thx), tly = (float)(ey - thy), tlz = (float)(ez - thz);
-  double ax = 0, ay = 0, az = 0;
-  const float f4 = (float)P.f4pi;
-  for (int base = 0; base < n_src; base += kTS) {
+  double acc[kTT][3];
+#pragma unroll
+  for (int u = 0; u < kTT; ++u) acc[u][0] = acc[u][1] = acc[u][2] = 0;
+  const double f4pi = P.f4pi;
+  // FP64 evaluation of segment id at target u (skip rule of
+  // calculate_vs_shift, src/tangle.c:567-569, for the tangle itself)
+  auto special = [&](int u, int id) {
+#pragma unroll
+    for (int v = 0; v < kTT; ++v) {
+      if (v != u) continue;
+      const int k = kk[v];
+      if (k < 0 || id < 0) return;
+      const int fw = S.fwd[id];
+      if (j == 0 && (id == k || fw == k)) return;
+      d3 r = ld3(pos, k);
+      if (j > 0) r = image_point(P, j - 1, r);
+      const double* sg = S.r1r2 + 6 * (size_t)id;
+      const d3 vv = seg_vel64(f4pi, mk3(sg[0], sg[1], sg[2]), mk3(sg[3], sg[4], sg[5]), r);
+      acc[v][0] += vv.x;
+      acc[v][1] += vv.y;
+      acc[v][2] += vv.z;
+    }
+  };
+  auto stage_one = [&](int m) -> SrcVals {
+    const int id = m < n_src ? order[m] : -1;
+    const int fw = id >= 0 ? S.fwd[id] : -1;
+    if (fw < 0) return src_none();
+    const double* sg = S.r1r2 + 6 * (size_t)id;
+    const double dxx = sg[3] - sg[0], dyy = sg[4] - sg[1], dzz = sg[5] - sg[2];
+    double far2 = fmax(16.0 * (dxx * dxx + dyy * dyy + dzz * dzz), P.near2);
+    if (j == 0) {
+      const d3 e = ld3(pos, fw);
+      if (e.x != sg[3] || e.y != sg[4] || e.z != sg[5]) far2 = 1e30;
+    }
+    return src_from(sg[0] - O.x, sg[1] - O.y, sg[2] - O.z, dxx, dyy, dzz, far2, id);
+  };
+  for (int sb = 0; sb < n_src; sb += kPSrc) {
     __syncthreads();
-    for (int q = threadIdx.x; q < kTS; q += kTB) {
-      int m = base + q;
-      int id = -1, fw = -1;
-      float4 hi = make_float4(0, 0, 0, 0), lo = make_float4(0, 0, 0, 0), d = make_float4(0, 0, 0, 0);
-      if (m < n_src) {
-        id = order ? order[m] : m;
-        fw = S.fwd[id];
-        if (fw >= 0) {
-          const double* src = S.r1r2 + 6 * id;
-          double dx = src[3] - src[0], dy = src[4] - src[1], dz = src[5] - src[2];
-          double px = src[0] - O.x, py = src[1] - O.y, pz = src[2] - O.z;
-          float hx = (float)px, hy = (float)py, hz = (float)pz;
-          // FP32 beyond max(4 |ds|, the near radius)
-          hi = make_float4(hx, hy, hz, (float)fmax(16.0 * (dx * dx + dy * dy + dz * dz), P.near2));
-          lo = make_float4((float)(px - hx), (float)(py - hy), (float)(pz - hz), 0.f);
-          d = make_float4((float)dx, (float)dy, (float)dz, 0.f);
+    for (int q = threadIdx.x; q < kPSrc / 2; q += kPB)
+      stage_pair(sh[q], stage_one(sb + 2 * q), stage_one(sb + 2 * q + 1));
+    __syncthreads();
+    // FP32 partial sums over 32 sources, each added into the FP64 sums
+    for (int q0 = 0; q0 < kPSrc / 2; q0 += 16) {
+      f2 b[kTT][3];
+#pragma unroll
+      for (int k = 0; k < kTT; ++k) b[k][0] = b[k][1] = b[k][2] = f2_splat(0.f);
+#pragma unroll 2
+      for (int q = q0; q < q0 + 16; ++q) pair_interact<false>(sh[q], T, b, special);
+#pragma unroll
+      for (int k = 0; k < kTT; ++k) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float lo, hi;
+          f2_unpack(b[k][c], lo, hi);
+          acc[k][c] += f4pi * ((double)lo + (double)hi);
         }
       }
-      sh_hi[q] = hi;
-      sh_lo[q] = lo;
-      sh_d[q] = d;
-      sh_id[q][0] = id;
-      sh_id[q][1] = fw;
-    }
-    __syncthreads();
-    if (!act) continue;
-    int cnt = min(kTS, n_src - base);
-    // FP32 partial sums over 32 sources, each flushed into the FP64 sum
-    for (int q0 = 0; q0 < cnt; q0 += 32) {
-      float bx = 0, by = 0, bz = 0;
-      int q1 = min(q0 + 32, cnt);
-      for (int q = q0; q < q1; ++q) {
-        const float4 a = sh_hi[q];
-        const float4 l = sh_lo[q];
-        const float4 d = sh_d[q];
-        float Rx = (a.x - thx) + (l.x - tlx);
-        float Ry = (a.y - thy) + (l.y - tly);
-        float Rz = (a.z - thz) + (l.z - tlz);
-        float R2 = fmaf(Rx, Rx, fmaf(Ry, Ry, Rz * Rz));
-        const int id = sh_id[q][0], fw = sh_id[q][1];
-        // skip rule of calculate_vs_shift (src/tangle.c:567-569) at any
-        // distance: across a periodic face a neighbour's segment is far
-        if (fw == -1 || id == skip || fw == skip) continue;
-        float vx, vy, vz;
-        if (R2 >= a.w && seg_vel32(f4, Rx, Ry, Rz, d.x, d.y, d.z, vx, vy, vz)) {
-          bx += vx; by += vy; bz += vz;
-        } else {
-          const double* src = S.r1r2 + 6 * id;
-          d3 v = seg_vel64(P.f4pi, mk3(src[0], src[1], src[2]), mk3(src[3], src[4], src[5]), r);
-          ax += v.x; ay += v.y; az += v.z;
-        }
-      }
-      ax += bx; ay += by; az += bz;
     }
   }
-  if (k >= 0) {
-    double* o = part + (size_t)j * 3 * stride + 3 * (size_t)k;
-    o[0] = act ? ax : 0; o[1] = act ? ay : 0; o[2] = act ? az : 0;
+#pragma unroll
+  for (int u = 0; u < kTT; ++u) {
+    const int i = base + threadIdx.x + kPB * u;
+    if (i >= n_t) continue;
+    double* o = part + (size_t)j * 3 * stride + 3 * (size_t)order[i];
+    const bool act = kk[u] >= 0;
+    o[0] = act ? acc[u][0] : 0;
+    o[1] = act ? acc[u][1] : 0;
+    o[2] = act ? acc[u][2] : 0;
   }
 }
 
@@ -245,18 +254,19 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
   dim3 grid((s->n + kTB - 1) / kTB, nimg + 1);
   SegTab S{s->seg64.as<double>(), s->segid.as<int>()};
   OvStatsAcc& st = ov_stats_tls();
-  cudaEventRecord(s->ev1, s->stream);
   if (s->P.precision == OV_PREC_MIXED) {
-    // spatially sorted order from the tree's key sort
+    // spatially sorted order from the tree's key sort (timed as the build)
     if (!ov_tree_build(s, pos, &s->tree)) return false;
-    k_direct_mixed<<<dim3((s->tree.n_nodes + kTB - 1) / kTB, nimg + 1), kTB, 0, s->stream>>>(
+    cudaEventRecord(s->ev1, s->stream);
+    k_direct_mixed_pairs<<<dim3((s->tree.n_nodes + kPTgt - 1) / kPTgt, nimg + 1), kPB, 0, s->stream>>>(
         s->P, S, s->tree.n_nodes, pos, s->status.as<int2>(), s->tree.perm.as<int>(), s->tree.n_nodes,
         s->n, s->img_part.as<double>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
-    // k_direct_mixed wrote part[j][k] for slots k in the sorted set only;
+    // k_direct_mixed_pairs wrote part[j][k] for slots k in the sorted set only;
     // EMPTY slots are never read by the epilogue, but zero them for hygiene
   } else {
+    cudaEventRecord(s->ev1, s->stream);
     k_direct64<<<grid, kTB, 0, s->stream>>>(s->P, S, s->n, nullptr, pos, s->status.as<int2>(),
                                             nullptr, s->n, s->img_part.as<double>());
     OV_LAUNCHED();
