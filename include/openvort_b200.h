@@ -380,6 +380,37 @@ typedef struct {
 } ov_batch_stats;
 int ov_batch_get_stats(ov_batch *b, ov_batch_stats *out);
 
+/* ----- adjoint of an RK4 trajectory with fixed topology -----
+ * Reverse-mode derivatives of the velocity and of nsteps x (update_tangle +
+ * rk4_step) with respect to the initial positions and the normal-fluid
+ * velocity vector (the "simple" flow of vn_conf, driving mutual friction).
+ * The reference has no derivatives; the forward dynamics are its own
+ * (update_velocity, src/tangle.c:583-684; rk4_step, src/vortex_dynamics.c:
+ * 58-121) with reconnection and remeshing off.  Scope: closed loops of free
+ * nodes (EMPTY slots allowed), open boundaries, no images, direct sum (the
+ * tree setting is ignored), superfluid and normal-fluid flows "no flow" or
+ * "simple".  Precision follows ov_set_precision for the forward velocities;
+ * the vector-Jacobian products are FP64.  Positions and cotangents are host
+ * arrays of 3*N doubles (slot order); vn is 3 doubles (NULL: keep the
+ * current vector, initially vn_conf's).  Branch decisions (hyperfriction
+ * threshold, cut-offs) are those of the forward values. */
+typedef struct ov_adjoint ov_adjoint;
+ov_adjoint *ov_adjoint_create(const struct tangle_state *tangle);
+void ov_adjoint_destroy(ov_adjoint *a);
+/* velocities at positions x */
+int ov_adjoint_velocity(ov_adjoint *a, const double *x, const double *vn, double t, double *v);
+/* x_bar = (dv/dx)^T v_bar and vn_bar = (dv/dvn)^T v_bar at positions x */
+int ov_adjoint_velocity_vjp(ov_adjoint *a, const double *x, const double *vn, double t,
+                            const double *v_bar, double *x_bar, double *vn_bar);
+/* nsteps RK4 steps from x0 at t0, positions checkpointed every
+ * checkpoint_every steps; x_final may be NULL */
+int ov_adjoint_forward(ov_adjoint *a, const double *x0, const double *vn, double t0, double dt,
+                       int nsteps, int checkpoint_every, double *x_final);
+/* cotangent of the last forward run's final positions -> cotangents of its
+ * initial positions and of vn (recomputing each block of steps from its
+ * checkpoint) */
+int ov_adjoint_backward(ov_adjoint *a, const double *x_final_bar, double *x0_bar, double *vn_bar);
+
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);

@@ -32,7 +32,8 @@ FUNCTIONS = [
     "ov_set_mixed_near_factor", "ov_get_mixed_near_factor", "ov_direct_points_noalloc",
     "ov_batch_create", "ov_batch_destroy", "ov_batch_update", "ov_batch_run",
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
-    "ov_batch_get_stats",
+    "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
+    "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -136,6 +137,14 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_batch_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
         "ov_batch_autotune": (C.c_int, [C.c_void_p, C.POINTER(BatchTuning)]),
         "ov_batch_get_stats": (C.c_int, [C.c_void_p, C.POINTER(BatchStats)]),
+        "ov_adjoint_create": (C.c_void_p, [T]),
+        "ov_adjoint_destroy": (None, [C.c_void_p]),
+        "ov_adjoint_velocity": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p]),
+        "ov_adjoint_velocity_vjp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                              C.c_void_p, C.c_void_p]),
+        "ov_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                         C.c_int, C.c_int, C.c_void_p]),
+        "ov_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

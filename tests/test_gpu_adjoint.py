@@ -1,0 +1,163 @@
+"""GPU: reverse-mode derivatives (ov_adjoint_*, openvort_b200.adjoint).
+
+Each gradient is checked against FP64 central finite differences of the
+forward computation of the same library:
+  - the velocity's vector-Jacobian product, along a random direction of the
+    positions and along the normal-fluid vector: relative error <= 1e-6;
+  - the gradient of |centroid - target|^2 + line length after 20 RK4 steps
+    of a ring with Kelvin waves, through the torch.autograd.Function, with
+    respect to the initial positions and vn: <= 1e-6 (FP64 forward), <= 1e-4
+    (mixed forward, whose trajectory differs from the FP64 one by ~1e-6);
+  - the checkpoint interval changes nothing (1e-13).
+"""
+import numpy as np
+import pytest
+
+from openvort_b200 import geometry as G
+from openvort_b200.tangle import Flow, Params
+
+pytestmark = pytest.mark.gpu
+
+N = 128
+R0 = 1e-2
+DL = 2 * np.pi * R0 / N
+# Hyperfriction switches on where the curvature exceeds max_curv_scale /
+# dl_max, so the dynamics are only piecewise smooth: dl_max = DL/4 puts that
+# threshold (1600 /cm) far above the ring's curvature (<= ~360 /cm), so no
+# node crosses it between the perturbed runs of the finite differences.
+# The branch itself is checked with hyperfriction active at every node.
+PARAMS = Params(kappa=9.97e-4, core_a=1e-8, use_mf=1, alpha=0.098, alpha_p=0.016, hyperfriction=1,
+                max_curv_scale=0.2, hyperalpha=0.5, dl_max=DL / 4,
+                vn=Flow("simple", {"external_v": (0.2, 0.0, 0.0)}), vs=Flow("no flow"))
+VN = np.array([0.2, 0.0, 0.0])
+DT, STEPS = 1e-5, 20       # omega dt ~ 0.3 for the grid-scale Kelvin waves
+TARGET = np.array([0.004, -0.002, 0.003])
+
+
+@pytest.fixture(scope="module")
+def ov():
+    import openvort_b200 as ov
+    lib = ov.load()
+    assert lib.ov_init(0) == 0, lib.ov_last_error_message()
+    return ov
+
+
+def kelvin_tangle():
+    pos = G.kelvin_ring(11, n=N, radius=R0, modes=(2, 16), sigma=1e-4)
+    return G.rings_to_tangle([pos], (-0.05,) * 3, (0.05,) * 3, "open")
+
+
+@pytest.fixture
+def adj(ov):
+    from openvort_b200.adjoint import Adjoint
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+    t = kelvin_tangle()
+    a = Adjoint(t)
+    yield t, a
+    a.close()
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+
+
+def rel(a, b):
+    return abs(a - b) / max(abs(b), 1e-300)
+
+
+def test_adjoint_velocity_matches_update_tangle(ov, adj):
+    t, a = adj
+    ref = t.copy()
+    ov.update_tangle(ref, 0.0)
+    v = a.velocity(t.pos, VN)
+    assert np.max(np.linalg.norm(v - ref.vels, axis=1) / np.linalg.norm(ref.vels, axis=1)) < 1e-13
+
+
+def test_velocity_vjp_with_hyperfriction_everywhere(ov):
+    """dl_max = 10 DL: threshold 20 /cm below every node's curvature."""
+    import dataclasses
+    from openvort_b200.adjoint import Adjoint
+    ov.configure(dataclasses.replace(PARAMS, dl_max=10 * DL), ov.OV_PREC_FP64)
+    t = kelvin_tangle()
+    a = Adjoint(t)
+    rng = np.random.default_rng(6)
+    g = rng.normal(size=(N, 3))
+    d = rng.normal(size=(N, 3)) * DL
+    xb, _ = a.velocity_vjp(t.pos, g, VN)
+    eps = 1e-5
+    fd = np.sum(g * (a.velocity(t.pos + eps * d, VN) - a.velocity(t.pos - eps * d, VN))) / (2 * eps)
+    assert rel(np.sum(xb * d), fd) < 1e-6
+    a.close()
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+
+
+def test_velocity_vjp_matches_central_differences(adj):
+    t, a = adj
+    rng = np.random.default_rng(5)
+    g = rng.normal(size=(N, 3))
+    d = rng.normal(size=(N, 3)) * DL
+    xb, vnb = a.velocity_vjp(t.pos, g, VN)
+    eps = 1e-5
+    fd = np.sum(g * (a.velocity(t.pos + eps * d, VN) - a.velocity(t.pos - eps * d, VN))) / (2 * eps)
+    assert rel(np.sum(xb * d), fd) < 1e-6
+    ev = 1e-3
+    for c in range(3):
+        e = np.zeros(3)
+        e[c] = ev
+        fdv = np.sum(g * (a.velocity(t.pos, VN + e) - a.velocity(t.pos, VN - e))) / (2 * ev)
+        assert abs(vnb[c] - fdv) <= 1e-6 * max(abs(fdv), np.max(np.abs(vnb)))
+
+
+def _loss_value(a, t, x0, vn):
+    import torch
+    from openvort_b200.adjoint import centroid_length_loss
+    xf = a.forward(x0, vn, 0.0, DT, STEPS, 8)
+    return float(centroid_length_loss(torch.from_numpy(xf), t.links[:, 0], t.active, TARGET))
+
+
+def _grads(a, t, every):
+    import torch
+    from openvort_b200.adjoint import centroid_length_loss, trajectory
+    x0 = torch.tensor(t.pos, dtype=torch.float64, requires_grad=True)
+    vn = torch.tensor(VN, dtype=torch.float64, requires_grad=True)
+    xf = trajectory(a, x0, vn, 0.0, DT, STEPS, every)
+    loss = centroid_length_loss(xf, t.links[:, 0], t.active, TARGET)
+    loss.backward()
+    return x0.grad.numpy().copy(), vn.grad.numpy().copy()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-6), (1, 1e-4)])
+def test_trajectory_gradient_matches_central_differences(ov, adj, precision, tol):
+    t, a = adj
+    ov.configure(PARAMS, precision)
+    gx, gv = _grads(a, t, every=8)
+    ov.configure(PARAMS, ov.OV_PREC_FP64)   # finite differences of the FP64 dynamics
+    rng = np.random.default_rng(9)
+    d = rng.normal(size=(N, 3)) * DL
+    eps = 1e-5
+    fd = (_loss_value(a, t, t.pos + eps * d, VN) - _loss_value(a, t, t.pos - eps * d, VN)) / (2 * eps)
+    assert rel(np.sum(gx * d), fd) < tol
+    ev = 1e-3
+    e = np.array([ev, 0.0, 0.0])
+    fdv = (_loss_value(a, t, t.pos, VN + e) - _loss_value(a, t, t.pos, VN - e)) / (2 * ev)
+    assert rel(gv[0], fdv) < tol
+
+
+def test_checkpoint_interval_changes_nothing(adj):
+    t, a = adj
+    g1, v1 = _grads(a, t, every=1)
+    for every in (7, 20, 64):
+        g, v = _grads(a, t, every=every)
+        assert np.max(np.abs(g - g1)) <= 1e-13 * np.max(np.abs(g1))
+        assert np.max(np.abs(v - v1)) <= 1e-13 * np.max(np.abs(v1))
+
+
+def test_adjoint_rejects_unsupported_tangles(ov, monkeypatch):
+    monkeypatch.setenv("OV_QUIET", "1")
+    lib = ov.load()
+    half = G.wall_half_ring()          # pinned ends on a mirror wall
+    assert not lib.ov_adjoint_create(half.ptr())
+    assert lib.ov_last_error() == ov._lib.OV_ERR_INVALID
+    lib.ov_clear_error()
+    per = G.rings_to_tangle([G.ring_points((0.05, 0.05, 0.05), (0, 0, 1), 0.01, 64)],
+                            (0, 0, 0), (0.1, 0.1, 0.1), "periodic-6")
+    assert not lib.ov_adjoint_create(per.ptr())
+    assert lib.ov_last_error() == ov._lib.OV_ERR_INVALID
+    lib.ov_clear_error()
