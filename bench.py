@@ -77,6 +77,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the direct-sum and batch lines")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--adjoint-steps", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -342,6 +343,114 @@ def bench_batch(args, ov, peak32: float):
     return out
 
 
+def bench_adjoint(args, ov):
+    """Adjoint of a 4096-point ring with Kelvin waves (modes 2-32, sigma
+    1e-4 cm), alpha = 0.098, alpha' = 0.016, v_ns = 0.2 cm/s: loss =
+    |centroid - target|^2 + line length after nsteps RK4 steps, checkpoints
+    every 32 steps.  Gradient with respect to the initial positions and v_ns,
+    FP64, against FP64 central differences along one seeded direction; the
+    same gradient with the mixed forward."""
+    import time as _t
+    import torch
+    from openvort_b200 import geometry as G
+    from openvort_b200.adjoint import Adjoint, centroid_length_loss, trajectory
+    from openvort_b200.tangle import Flow, Params
+    n, R0 = 4096, 1e-2
+    dl = 2 * np.pi * R0 / n
+    # grid-scale Kelvin waves: omega ~ 2e7 /s at this spacing, so RK4 needs
+    # dt ~ 5e-8 s (omega dt ~ 1)
+    dt, steps, every = 5e-8, args.adjoint_steps, 32
+    p = Params(kappa=9.97e-4, core_a=1e-8, use_mf=1, alpha=0.098, alpha_p=0.016, hyperfriction=1,
+               max_curv_scale=0.2, hyperalpha=0.5, dl_max=dl / 2, use_bh=0,
+               vn=Flow("simple", {"external_v": (0.2, 0.0, 0.0)}), vs=Flow("no flow"))
+    t = G.rings_to_tangle([G.kelvin_ring(args.seed + 5, n=n, radius=R0, modes=(2, 32), sigma=1e-4)],
+                          (-0.05,) * 3, (0.05,) * 3, "open")
+    vn0 = np.array([0.2, 0.0, 0.0])
+    target = np.array([0.0, 0.0, 0.01])
+    fwd = t.links[:, 0]
+
+    def grads(prec):
+        ov.configure(p, prec)
+        a = Adjoint(t)
+        x0 = torch.tensor(t.pos, dtype=torch.float64, requires_grad=True)
+        vn = torch.tensor(vn0, dtype=torch.float64, requires_grad=True)
+        t0 = _t.perf_counter()
+        xf = trajectory(a, x0, vn, 0.0, dt, steps, every)
+        t1 = _t.perf_counter()
+        loss = centroid_length_loss(xf, fwd, t.active, target)
+        loss.backward()
+        t2 = _t.perf_counter()
+        return a, x0.grad.numpy().copy(), vn.grad.numpy().copy(), t1 - t0, t2 - t1
+
+    a, gx, gv, tf, tb = grads(ov.OV_PREC_FP64)
+    rng = np.random.default_rng(args.seed + 6)
+    d = rng.normal(size=(n, 3)) * dl
+    eps = 1e-5
+
+    def lval(x0, vn):
+        xf = a.forward(x0, vn, 0.0, dt, steps, every)
+        return float(centroid_length_loss(torch.from_numpy(xf), fwd, t.active, target))
+    fd = (lval(t.pos + eps * d, vn0) - lval(t.pos - eps * d, vn0)) / (2 * eps)
+    e = np.array([1e-3, 0.0, 0.0])
+    fdv = (lval(t.pos, vn0 + e) - lval(t.pos, vn0 - e)) / 2e-3
+    a.close()
+    # Velocity-level check at this resolution.  The reference's colinearity
+    # cut-off (zero contribution when |cos - 1| < 1e-8) makes the velocity
+    # discontinuous where a segment's extension passes near a target: such
+    # nodes give finite differences that change with the step.  With the
+    # cotangent kept off them (and their stencil neighbours) the vector-
+    # Jacobian product is compared with the finite differences.
+    ov.configure(p, ov.OV_PREC_FP64)
+    av = Adjoint(t)
+    jv = {e_: (av.velocity(t.pos + e_ * d, vn0) - av.velocity(t.pos - e_ * d, vn0)) / (2 * e_)
+          for e_ in (1e-5, 1e-6)}
+    scale = np.linalg.norm(jv[1e-5], axis=1)
+    bad = np.linalg.norm(jv[1e-6] - jv[1e-5], axis=1) > 1e-6 * scale
+    mask = bad.copy()
+    for sh in (-2, -1, 1, 2):
+        mask |= np.roll(bad, sh)
+    gm = rng.normal(size=(n, 3))
+    gm[mask] = 0
+    xbm, _ = av.velocity_vjp(t.pos, gm, vn0)
+    fdm = float(np.sum(gm * jv[1e-5]))
+    vel_masked = abs(float(np.sum(xbm * d)) - fdm) / abs(fdm)
+    av.close()
+    # Trajectory-level check at the same resolution and step count with
+    # smaller waves (sigma = 1e-7 cm): their slopes (~3e-4) stay below the
+    # ring's own chord angle at the nearest segments, so no pair reaches the
+    # cut-off and the finite differences are well defined
+    ts = G.rings_to_tangle([G.kelvin_ring(args.seed + 5, n=n, radius=R0, modes=(2, 32), sigma=1e-7)],
+                           (-0.05,) * 3, (0.05,) * 3, "open")
+    a2 = Adjoint(ts)
+    x0t = torch.tensor(ts.pos, dtype=torch.float64, requires_grad=True)
+    vnt = torch.tensor(vn0, dtype=torch.float64, requires_grad=True)
+    xf2 = trajectory(a2, x0t, vnt, 0.0, dt, steps, every)
+    centroid_length_loss(xf2, fwd, ts.active, target).backward()
+
+    def lval2(x0, vn):
+        xf = a2.forward(x0, vn, 0.0, dt, steps, every)
+        return float(centroid_length_loss(torch.from_numpy(xf), fwd, ts.active, target))
+    fd2 = (lval2(ts.pos + eps * d, vn0) - lval2(ts.pos - eps * d, vn0)) / (2 * eps)
+    fd2v = (lval2(ts.pos, vn0 + e) - lval2(ts.pos, vn0 - e)) / 2e-3
+    smooth_pos = abs(float(np.sum(x0t.grad.numpy() * d)) - fd2) / abs(fd2)
+    smooth_vns = abs(float(vnt.grad.numpy()[0]) - fd2v) / abs(fd2v)
+    a2.close()
+    am, gxm, gvm, tfm, tbm = grads(ov.OV_PREC_MIXED)
+    am.close()
+    ov.configure(p, ov.OV_PREC_FP64)
+    ad = float(np.sum(gx * d))
+    return {"workload": f"ring R=1e-2 cm, {n} points, Kelvin modes 2-32 (sigma 1e-4 cm), {steps} RK4 steps "
+                        f"dt={dt}, checkpoints every {every}", "points": n, "steps": steps,
+            "forward_s": tf, "backward_s": tb, "mixed_forward_s": tfm, "mixed_backward_s": tbm,
+            "fd_rel_err_positions": abs(ad - fd) / abs(fd), "fd_rel_err_vns": abs(gv[0] - fdv) / abs(fdv),
+            "mixed_fd_rel_err_positions": abs(float(np.sum(gxm * d)) - fd) / abs(fd),
+            "mixed_fd_rel_err_vns": abs(gvm[0] - fdv) / abs(fdv),
+            "velocity_vjp_fd_rel_err_masked": vel_masked, "discontinuous_nodes": int(bad.sum()),
+            "fd_rel_err_positions_small_waves": smooth_pos, "fd_rel_err_vns_small_waves": smooth_vns,
+            "note": "fd_rel_err_* at 4096 points include the jumps of the reference's colinearity "
+                    "cut-off crossed between the perturbed runs"}
+
+
 def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
@@ -476,10 +585,11 @@ def main():
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
 
-    direct = batch = None
+    direct = batch = adjoint = None
     if not args.no_extra:
         direct = bench_direct(args, ov, peak32.value, peak64.value)
         batch = bench_batch(args, ov, peak32.value)
+        adjoint = bench_adjoint(args, ov)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -522,6 +632,7 @@ def main():
                          "tree_build_share_of_step": build_share},
             "direct_22k": direct,
             "batch_4096": batch,
+            "adjoint_4096": adjoint,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -22,6 +22,7 @@
 // sweep recomputes one block of steps from its checkpoint, then runs back
 // through it, recomputing each step's stage positions (y1..y3) and taking
 // the four stage VJPs.
+#include <algorithm>
 #include <vector>
 
 #include "ov_internal.h"
@@ -192,19 +193,20 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_targets(double f4pi, const doubl
                                                         const int2* __restrict__ links,
                                                         const int2* __restrict__ status,
                                                         const double* __restrict__ gnl, double* xbar,
-                                                        int n) {
+                                                        int n, int chunk) {
   __shared__ double sh[kVT][6];
   __shared__ int sid[kVT][2];
+  const int s_lo = blockIdx.y * chunk, s_hi = min(n, s_lo + chunk);   // this block's sources
   const int k = blockIdx.x * kVT + threadIdx.x;
   const bool act = k < n && status[k].x == OV_FREE;
   const d3 r = act ? ld3(pos, k) : mk3(0, 0, 0);
   const d3 g = act ? ld3(gnl, k) : mk3(0, 0, 0);
   d3 acc = mk3(0, 0, 0);
-  for (int base = 0; base < n; base += kVT) {
+  for (int base = s_lo; base < s_hi; base += kVT) {
     __syncthreads();
     const int m = base + threadIdx.x;
     int f = -1;
-    if (m < n && status[m].x != OV_EMPTY) f = links[m].x;
+    if (m < s_hi && status[m].x != OV_EMPTY) f = links[m].x;
     d3 a = mk3(0, 0, 0), b = a;
     if (f >= 0) {
       a = ld3(pos, m);
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_targets(double f4pi, const doubl
     sid[threadIdx.x][1] = f;
     __syncthreads();
     if (!act) continue;
-    const int cnt = min(kVT, n - base);
+    const int cnt = min(kVT, s_hi - base);
     for (int q = 0; q < cnt; ++q) {
       const int id = sid[q][0], fw = sid[q][1];
       if (fw < 0 || id == k || fw == k) continue;
@@ -238,19 +240,20 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_segments(double f4pi, const doub
                                                          const int2* __restrict__ links,
                                                          const int2* __restrict__ status,
                                                          const double* __restrict__ gnl, double* xbar,
-                                                         int n) {
+                                                         int n, int chunk) {
   __shared__ double sh[kVT][6];   // target position and its cotangent
   __shared__ int sid[kVT];
+  const int t_lo = blockIdx.y * chunk, t_hi = min(n, t_lo + chunk);   // this block's targets
   const int m = blockIdx.x * kVT + threadIdx.x;
   int f = -1;
   if (m < n && status[m].x != OV_EMPTY) f = links[m].x;
   const d3 r1 = f >= 0 ? ld3(pos, m) : mk3(0, 0, 0);
   const d3 r2 = f >= 0 ? ld3(pos, f) : mk3(0, 0, 0);
   d3 a1 = mk3(0, 0, 0), a2 = a1;
-  for (int base = 0; base < n; base += kVT) {
+  for (int base = t_lo; base < t_hi; base += kVT) {
     __syncthreads();
     const int k = base + threadIdx.x;
-    const bool t_ok = k < n && status[k].x == OV_FREE;
+    const bool t_ok = k < t_hi && status[k].x == OV_FREE;
     const d3 r = t_ok ? ld3(pos, k) : mk3(0, 0, 0);
     const d3 g = t_ok ? ld3(gnl, k) : mk3(0, 0, 0);
     sh[threadIdx.x][0] = r.x; sh[threadIdx.x][1] = r.y; sh[threadIdx.x][2] = r.z;
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_segments(double f4pi, const doub
     sid[threadIdx.x] = t_ok ? k : -1;
     __syncthreads();
     if (f < 0) continue;
-    const int cnt = min(kVT, n - base);
+    const int cnt = min(kVT, t_hi - base);
     for (int q = 0; q < cnt; ++q) {
       const int kk = sid[q];
       if (kk < 0 || kk == m || kk == f) continue;
@@ -304,6 +307,23 @@ struct ov_adjoint {
 namespace {
 
 int blocks(long long m, int t = 256) { return (int)((m + t - 1) / t); }
+
+// all-pairs passes: split the inner range so that a small tangle still
+// fills the GPU (about 4 blocks per SM); returns the range per split
+int pair_chunk(int n, int* splits) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 1;
+  }
+  const int bx = blocks(n, kVT);
+  int sp = std::min(32, std::max(1, (4 * sms + bx - 1) / bx));
+  int chunk = (n + sp - 1) / sp;
+  chunk = (chunk + kVT - 1) / kVT * kVT;
+  *splits = std::max(1, (n + chunk - 1) / chunk);
+  return chunk;
+}
 
 bool flow_ok(const OvFlow& f) { return f.kind == OVF_NONE || f.kind == OVF_SIMPLE; }
 
@@ -365,11 +385,14 @@ bool velocity_vjp(ov_adjoint* a, const double* x, const double* g, double* ybar)
       a->gnl.as<double>(), a->vnbar.as<double>(), n);
   OV_LAUNCHED();
   if (!s->P.lia_only) {
-    k_bs_vjp_targets<<<blocks(n, kVT), kVT, 0, s->stream>>>(s->P.f4pi, x, s->links.as<int2>(),
-                                                             s->status.as<int2>(), a->gnl.as<double>(), ybar, n);
+    int splits = 1;
+    const int chunk = pair_chunk(n, &splits);
+    const dim3 grid(blocks(n, kVT), splits);
+    k_bs_vjp_targets<<<grid, kVT, 0, s->stream>>>(s->P.f4pi, x, s->links.as<int2>(), s->status.as<int2>(),
+                                                  a->gnl.as<double>(), ybar, n, chunk);
     OV_LAUNCHED();
-    k_bs_vjp_segments<<<blocks(n, kVT), kVT, 0, s->stream>>>(s->P.f4pi, x, s->links.as<int2>(),
-                                                              s->status.as<int2>(), a->gnl.as<double>(), ybar, n);
+    k_bs_vjp_segments<<<grid, kVT, 0, s->stream>>>(s->P.f4pi, x, s->links.as<int2>(), s->status.as<int2>(),
+                                                   a->gnl.as<double>(), ybar, n, chunk);
     OV_LAUNCHED();
   }
   OV_TRY_CUDA(cudaGetLastError());

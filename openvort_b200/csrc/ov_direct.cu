@@ -15,6 +15,8 @@
 // rounded once) and evaluated two per f32x2 instruction (ov_pair.cuh); near
 // or borderline-colinear pairs fall back to seg_vel64 from the FP64 table;
 // sums accumulate in FP64.
+#include <algorithm>
+
 #include "ov_internal.h"
 #include "ov_pair.cuh"
 
@@ -43,12 +45,14 @@ __global__ void k_segtab(OvParams P, const double* __restrict__ pos, const int2*
 }
 
 // Targets: either node slots (pts == nullptr: slot k, status-filtered) or
-// explicit points.  Sources: all slots, or the list `only`.
+// explicit points.  Sources: all slots, or the list `only`; split z of the
+// grid takes sources [z chunk, (z + 1) chunk) and writes its own partial
+// sums part[z][image][target].
 __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_src, const int* only,
                                                   const double* __restrict__ tpos,
                                                   const int2* __restrict__ tstatus,
                                                   const int* __restrict__ tskip, int n_t,
-                                                  double* __restrict__ part) {
+                                                  double* __restrict__ part, int chunk) {
   __shared__ double sh_r[kTS][6];
   __shared__ int sh_id[kTS][2];
   const int j = blockIdx.y;  // 0: the tangle itself, j >= 1: image j-1
@@ -64,12 +68,13 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
   }
   double ax = 0, ay = 0, az = 0;
   const double f4pi = P.f4pi;
-  for (int base = 0; base < n_src; base += kTS) {
+  const int s_lo = blockIdx.z * chunk, s_hi = min(n_src, s_lo + chunk);
+  for (int base = s_lo; base < s_hi; base += kTS) {
     __syncthreads();
     for (int q = threadIdx.x; q < kTS; q += kTB) {
       int m = base + q;
       int id = -1, fw = -1;
-      if (m < n_src) {
+      if (m < s_hi) {
         id = only ? only[m] : m;
         fw = S.fwd[id];
         const double* src = S.r1r2 + 6 * id;
@@ -81,7 +86,7 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
     }
     __syncthreads();
     if (!act) continue;
-    int cnt = min(kTS, n_src - base);
+    int cnt = min(kTS, s_hi - base);
     for (int q = 0; q < cnt; ++q) {
       int id = sh_id[q][0], fw = sh_id[q][1];
       // skip rule of calculate_vs_shift (src/tangle.c:567-569)
@@ -91,12 +96,9 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
       ax += v.x; ay += v.y; az += v.z;
     }
   }
-  if (act) {
-    double* o = part + (size_t)j * 3 * n_t + 3 * (size_t)k;
-    o[0] = ax; o[1] = ay; o[2] = az;
-  } else if (k < n_t) {
-    double* o = part + (size_t)j * 3 * n_t + 3 * (size_t)k;
-    o[0] = 0; o[1] = 0; o[2] = 0;
+  if (k < n_t) {
+    double* o = part + ((size_t)blockIdx.z * gridDim.y + j) * 3 * n_t + 3 * (size_t)k;
+    o[0] = act ? ax : 0; o[1] = act ? ay : 0; o[2] = act ? az : 0;
   }
 }
 
@@ -117,7 +119,7 @@ constexpr int kPSrc = 128;          // sources per shared-memory tile (kPSrc / 2
 
 __global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
     OvParams P, SegTab S, int n_src, const double* __restrict__ pos, const int2* __restrict__ tstatus,
-    const int* __restrict__ order, int n_t, int stride, double* __restrict__ part) {
+    const int* __restrict__ order, int n_t, int stride, double* __restrict__ part, int chunk) {
   __shared__ PairSrc<false> sh[kPSrc / 2];
   const int j = blockIdx.y;   // 0: the tangle itself, j >= 1: image j-1
   const int base = blockIdx.x * kPTgt;
@@ -161,8 +163,9 @@ __global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
       acc[v][2] += vv.z;
     }
   };
+  const int s_lo = blockIdx.z * chunk, s_hi = min(n_src, s_lo + chunk);
   auto stage_one = [&](int m) -> SrcVals {
-    const int id = m < n_src ? order[m] : -1;
+    const int id = m < s_hi ? order[m] : -1;
     const int fw = id >= 0 ? S.fwd[id] : -1;
     if (fw < 0) return src_none();
     const double* sg = S.r1r2 + 6 * (size_t)id;
@@ -174,7 +177,7 @@ __global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
     }
     return src_from(sg[0] - O.x, sg[1] - O.y, sg[2] - O.z, dxx, dyy, dzz, far2, id);
   };
-  for (int sb = 0; sb < n_src; sb += kPSrc) {
+  for (int sb = s_lo; sb < s_hi; sb += kPSrc) {
     __syncthreads();
     for (int q = threadIdx.x; q < kPSrc / 2; q += kPB)
       stage_pair(sh[q], stage_one(sb + 2 * q), stage_one(sb + 2 * q + 1));
@@ -201,7 +204,7 @@ __global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
   for (int u = 0; u < kTT; ++u) {
     const int i = base + threadIdx.x + kPB * u;
     if (i >= n_t) continue;
-    double* o = part + (size_t)j * 3 * stride + 3 * (size_t)order[i];
+    double* o = part + ((size_t)blockIdx.z * gridDim.y + j) * 3 * stride + 3 * (size_t)order[i];
     const bool act = kk[u] >= 0;
     o[0] = act ? acc[u][0] : 0;
     o[1] = act ? acc[u][1] : 0;
@@ -210,16 +213,20 @@ __global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
 }
 
 // v_nl = part[0]; v_img = sum_j part[j] in image order (src/tangle.c:627-638);
-// mirror images reflect their velocity (src/tangle.c:633-634)
+// mirror images reflect their velocity (src/tangle.c:633-634).  With source
+// splits, each image's partial sums are added split by split, in order.
 __global__ void k_reduce_images(OvParams P, const double* __restrict__ part, int n_t,
-                                double* v_nl, double* v_img) {
+                                double* v_nl, double* v_img, int splits) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n_t) return;
+  const size_t img_stride = 3 * (size_t)n_t, split_stride = img_stride * (P.n_img + 1);
   d3 a = ld3(part, k);
+  for (int z = 1; z < splits; ++z) a = a + ld3(part + z * split_stride, k);
   if (v_nl) st3(v_nl, k, a);
   d3 s = mk3(0, 0, 0);
   for (int j = 1; j <= P.n_img; ++j) {
-    d3 v = ld3(part + (size_t)j * 3 * n_t, k);
+    d3 v = ld3(part + (size_t)j * img_stride, k);
+    for (int z = 1; z < splits; ++z) v = v + ld3(part + z * split_stride + (size_t)j * img_stride, k);
     int face = P.img[j - 1][3];
     if (face > -1) v = mirror_dir(v, face);
     s = s + v;
@@ -245,36 +252,58 @@ static bool ensure_segtab(ov_state_impl* s, const double* pos) {
   return true;
 }
 
+// Source splits for a grid of `blocks` target blocks: enough that a small
+// tangle still fills the GPU (about 4 blocks per SM), each split a whole
+// number of tiles of `tile` sources; returns the sources per split.
+static int source_chunk(int n_src, long long blocks, int tile, int* splits) {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 1;
+  }
+  long long want = (4LL * sms + blocks - 1) / std::max(1LL, blocks);
+  int sp = (int)std::min<long long>(16, std::max<long long>(1, want));
+  int chunk = (n_src + sp - 1) / sp;
+  chunk = std::max(tile, (chunk + tile - 1) / tile * tile);
+  *splits = std::max(1, (n_src + chunk - 1) / chunk);
+  return chunk;
+}
+
 bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* v_img) {
   if (s->n == 0) return true;
   if (!ensure_segtab(s, pos)) return false;
   int nimg = s->P.n_img;
-  size_t bytes = sizeof(double) * 3 * (size_t)s->n * (nimg + 1);
-  if (!s->img_part.reserve(bytes)) return false;
-  dim3 grid((s->n + kTB - 1) / kTB, nimg + 1);
   SegTab S{s->seg64.as<double>(), s->segid.as<int>()};
   OvStatsAcc& st = ov_stats_tls();
+  int splits = 1;
   if (s->P.precision == OV_PREC_MIXED) {
     // spatially sorted order from the tree's key sort (timed as the build)
     if (!ov_tree_build(s, pos, &s->tree)) return false;
+    const int bx = (s->tree.n_nodes + kPTgt - 1) / kPTgt;
+    const int chunk = source_chunk(s->tree.n_nodes, (long long)bx * (nimg + 1), kPSrc, &splits);
+    if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;
     cudaEventRecord(s->ev1, s->stream);
-    k_direct_mixed_pairs<<<dim3((s->tree.n_nodes + kPTgt - 1) / kPTgt, nimg + 1), kPB, 0, s->stream>>>(
+    k_direct_mixed_pairs<<<dim3(bx, nimg + 1, splits), kPB, 0, s->stream>>>(
         s->P, S, s->tree.n_nodes, pos, s->status.as<int2>(), s->tree.perm.as<int>(), s->tree.n_nodes,
-        s->n, s->img_part.as<double>());
+        s->n, s->img_part.as<double>(), chunk);
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
     // k_direct_mixed_pairs wrote part[j][k] for slots k in the sorted set only;
     // EMPTY slots are never read by the epilogue, but zero them for hygiene
   } else {
+    const int bx = (s->n + kTB - 1) / kTB;
+    const int chunk = source_chunk(s->n, (long long)bx * (nimg + 1), kTS, &splits);
+    if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;
     cudaEventRecord(s->ev1, s->stream);
-    k_direct64<<<grid, kTB, 0, s->stream>>>(s->P, S, s->n, nullptr, pos, s->status.as<int2>(),
-                                            nullptr, s->n, s->img_part.as<double>());
+    k_direct64<<<dim3(bx, nimg + 1, splits), kTB, 0, s->stream>>>(
+        s->P, S, s->n, nullptr, pos, s->status.as<int2>(), nullptr, s->n, s->img_part.as<double>(), chunk);
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
   }
   cudaEventRecord(s->ev2, s->stream);
   k_reduce_images<<<(s->n + 255) / 256, 256, 0, s->stream>>>(s->P, s->img_part.as<double>(), s->n,
-                                                              v_nl, v_img);
+                                                              v_nl, v_img, splits);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   (void)st;
@@ -293,14 +322,14 @@ bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const doubl
   SegTab S{s->seg64.as<double>(), s->segid.as<int>()};
   int n_src = only ? n_only : s->n;
   k_direct64<<<grid, kTB, 0, s->stream>>>(s->P, S, n_src, only, pts, nullptr, skip, npts,
-                                          s->img_part.as<double>());
+                                          s->img_part.as<double>(), std::max(1, n_src));
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   // out_nl = part[0]; out_img = image sum in table order (src/tangle.c:624-638)
   OvParams P = s->P;
   P.n_img = nimg;
   k_reduce_images<<<(npts + 255) / 256, 256, 0, s->stream>>>(P, s->img_part.as<double>(), npts,
-                                                              out_nl, out_img);
+                                                              out_nl, out_img, 1);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   return true;
@@ -327,9 +356,10 @@ bool ov_direct_points_scratch(cudaStream_t st, const OvParams& P, const double* 
     OV_LAUNCHED();
   }
   dim3 grid((npts + kTB - 1) / kTB, P.n_img + 1);
-  k_direct64<<<grid, kTB, 0, st>>>(P, SegTab{seg, fwd}, n, nullptr, pts, nullptr, skip, npts, part);
+  k_direct64<<<grid, kTB, 0, st>>>(P, SegTab{seg, fwd}, n, nullptr, pts, nullptr, skip, npts, part,
+                                   std::max(1, n));
   OV_LAUNCHED();
-  k_reduce_images<<<(npts + 255) / 256, 256, 0, st>>>(P, part, npts, out, img);
+  k_reduce_images<<<(npts + 255) / 256, 256, 0, st>>>(P, part, npts, out, img, 1);
   OV_LAUNCHED();
   k_add3<<<(3 * npts + 255) / 256, 256, 0, st>>>(out, img, out, npts);
   OV_LAUNCHED();
