@@ -153,34 +153,23 @@ class Clocks:
 
 
 def dist_setup(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    dist = None
-    if world > 1:
+    from openvort_b200 import dist as D
+    r = D.setup()
+    if r.world == 1:
         import torch
-        import torch.distributed as dist_mod
-        torch.cuda.set_device(local)
-        dist_mod.init_process_group("nccl", device_id=torch.device("cuda", local),
-                                    timeout=__import__("datetime").timedelta(seconds=600))
-        dist = dist_mod
-    return world, rank, local, dist
+        if torch.cuda.is_available():
+            r.device = f"cuda:{r.local}"
+    return r.world, r.rank, r.local, r
 
 
-def max_over_ranks(dist, x: float) -> float:
-    if dist is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+def max_over_ranks(r, x: float) -> float:
+    from openvort_b200 import dist as D
+    return D.max_over_ranks(r, x)
 
 
-def barrier(dist):
-    import torch
-    if dist is not None:
-        dist.barrier()
-    torch.cuda.synchronize()
+def barrier(r):
+    from openvort_b200 import dist as D
+    D.barrier(r)
 
 
 # ---------------------------------------------------------------- CPU side
@@ -457,8 +446,8 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference_arm(args, world, rank)
-        if dist is not None:
-            dist.destroy_process_group()
+        from openvort_b200 import dist as D
+        D.close(dist)
         return
 
     import torch
@@ -470,7 +459,8 @@ def main():
         raise SystemExit(f"libov_gpu: {lib.ov_last_error_message().decode()}")
     torch.cuda.set_device(local)
     p = params(args.theta)
-    tangle, n_rings = make_tangle(args.points, args.seed + 1000 * rank)
+    from openvort_b200.dist import rank_seed
+    tangle, n_rings = make_tangle(args.points, rank_seed(args.seed, rank))
     n = int(tangle.active.sum())
 
     # ---------------- device-resident timing, mixed precision
@@ -639,8 +629,8 @@ def main():
             "clocks": clk,
         }
         print(json.dumps(line))
-    if dist is not None:
-        dist.destroy_process_group()
+    from openvort_b200 import dist as D
+    D.close(dist)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,83 @@
+"""Multi-process rank plumbing (openvort_b200.dist) on CPU with gloo,
+world size 2: the timing collectives of multi-GPU runs, the per-rank seeds
+of the independent tangles, and a rank that never joins a collective
+ending the other's with an error (host-side failure detection)."""
+import os
+import socket
+
+import pytest
+
+torch = pytest.importorskip("torch")
+mp = pytest.importorskip("torch.multiprocessing")
+
+
+def _free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q, mode):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    from openvort_b200 import dist as D
+    try:
+        r = D.setup("gloo", timeout_s=5.0)
+        if mode == "collectives":
+            D.barrier(r)
+            mx = D.max_over_ranks(r, 1.5 + rank)
+            sm = D.sum_over_ranks(r, 1.0 + rank)
+            q.put((rank, mx, sm, D.rank_seed(2024, rank)))
+        elif mode == "missing_rank":
+            if rank == 1:
+                q.put((rank, "left"))           # leaves between steps, joins nothing
+            else:
+                try:
+                    D.max_over_ranks(r, 1.0)
+                    q.put((rank, "no error"))
+                except Exception as e:          # the group's timeout ends the collective
+                    q.put((rank, "error", type(e).__name__))
+        if mode != "missing_rank":
+            D.close(r)
+    except Exception as e:   # pragma: no cover - reported to the parent
+        q.put((rank, "exception", repr(e)))
+
+
+def _run(mode, world=2, timeout=60):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q, mode)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=timeout) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=timeout)
+        if p.is_alive():
+            p.kill()
+    return sorted(out)
+
+
+def test_single_process_needs_no_group(monkeypatch):
+    from openvort_b200 import dist as D
+    monkeypatch.delenv("WORLD_SIZE", raising=False)
+    r = D.setup()
+    assert r.world == 1 and r.pg is None
+    assert D.max_over_ranks(r, 3.0) == 3.0
+    D.barrier(r)
+
+
+def test_timing_collectives_world_2():
+    out = _run("collectives")
+    assert [o[0] for o in out] == [0, 1]
+    for rank, mx, sm, seed in out:
+        assert mx == 2.5          # the slowest rank's time
+        assert sm == 3.0
+        assert seed == 2024 + 1000 * rank
+    assert out[0][3] != out[1][3]  # every rank its own tangle
+
+
+def test_rank_that_never_joins_ends_the_collective_with_an_error():
+    out = _run("missing_rank")
+    assert out[1][:2] == (1, "left")
+    assert out[0][0] == 0 and out[0][1] == "error"
