@@ -411,6 +411,27 @@ int ov_adjoint_forward(ov_adjoint *a, const double *x0, const double *vn, double
  * checkpoint) */
 int ov_adjoint_backward(ov_adjoint *a, const double *x_final_bar, double *x0_bar, double *vn_bar);
 
+/* ----- vortex-vortex reconnection with the pair search on the GPU -----
+ * The reference's pair loop (reconnect, src/vortex_dynamics.c:216-313)
+ * tests all N^2/2 node pairs.  The tests that cannot change during a pass
+ * (neither node empty or pinned, not linked, distance after the periodic
+ * wrap <= rec_dist, both tangents >= 0.5 long, tangents at an angle above
+ * rec_angle) are done here by a GPU grid search in the reference's FP64
+ * operations.  tangle->tangents must be current.
+ * ov_reconnect_candidates writes up to max_pairs pairs (k, l), k < l, as
+ * 2 ints each, in the loop's order (k, then l ascending), and returns how
+ * many there are (or -OV_ERR_*).  ov_reconnect_vortices then runs the rest
+ * of the loop on the host in that order: the links and sit-out flags
+ * (tangle->recalculate) of the pass so far, the approach test with
+ * update_velocity of both nodes (direct sum, as the reference), and
+ * do_reconnection (src/vortex_dynamics.c:317-364).  Its result is the
+ * reference loop's: same links, flags, velocities written and count
+ * (returned, or -OV_ERR_*).  Wall reconnections, small-loop removal and
+ * domain cleanup stay with the reference's reconnect(). */
+int ov_reconnect_candidates(const struct tangle_state *tangle, double rec_dist, double rec_angle,
+                            int *pairs, int max_pairs);
+int ov_reconnect_vortices(struct tangle_state *tangle, double t, double rec_dist, double rec_angle);
+
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);

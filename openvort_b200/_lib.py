@@ -34,6 +34,7 @@ FUNCTIONS = [
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
     "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward",
+    "ov_reconnect_candidates", "ov_reconnect_vortices",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -145,6 +146,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                          C.c_int, C.c_int, C.c_void_p]),
         "ov_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ov_reconnect_candidates": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p, C.c_int]),
+        "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -214,6 +214,17 @@ class Ref:
         self.lib.refh_rk4_step(out.ptr(), C.c_double(time), C.c_double(dt))
         return out
 
+    def reconnect(self, t: HostTangle, p: Params, time, rec_dist, rec_angle):
+        """The reference's reconnect (src/vortex_dynamics.c:140-313) on a copy
+        whose tangents and normals are current; returns (copy, count)."""
+        self.configure(p)
+        out = self._copy(t)
+        f = self.lib.reconnect
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, C.c_double, C.c_double, C.c_double]
+        n = f(C.cast(out.ptr(), C.c_void_p), time, rec_dist, rec_angle)
+        return out, n
+
     def segments_at(self, t: HostTangle, p: Params, pts, skip=None) -> np.ndarray:
         self.configure(p)
         tt = self._copy(t)

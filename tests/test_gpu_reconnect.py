@@ -1,0 +1,128 @@
+"""GPU: vortex-vortex reconnection with the GPU pair search
+(ov_reconnect_candidates, ov_reconnect_vortices) against the reference's own
+reconnect() compiled from its sources (oracle/_ref): the same links,
+sit-out flags, count and velocities, on crossing rings (open box) and on
+dense random tangles (open and periodic); the candidate list against a
+brute-force scan of the reference's tests in numpy."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from openvort_b200 import geometry as G
+from openvort_b200.tangle import Flow, Params
+from oracle.oracle import Ref, have_ref
+
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_ref(), reason="oracle/_ref not built")]
+
+PARAMS = Params(kappa=9.97e-4, core_a=1e-8, use_mf=1, alpha=0.1, alpha_p=0.01, hyperfriction=0,
+                dl_max=1e-3, vn=Flow("simple", {"external_v": (0.1, 0.0, 0.0)}), vs=Flow("no flow"))
+REC_ANGLE = 0.087
+
+
+@pytest.fixture(scope="module")
+def ov():
+    import openvort_b200 as ov
+    lib = ov.load()
+    assert lib.ov_init(0) == 0, lib.ov_last_error_message()
+    return ov
+
+
+def crossing_rings(seed, n=200, R=1e-2):
+    """ring A in the xy plane; ring B in a random plane through a point a
+    fraction of a spacing off A's node at (R, 0, 0)"""
+    rng = np.random.default_rng(seed)
+    a = G.ring_points((0, 0, 0), (0, 0, 1), R, n)
+    nb = rng.normal(size=3)
+    nb /= np.linalg.norm(nb)
+    u = np.cross(nb, rng.normal(size=3))
+    u /= np.linalg.norm(u)
+    gap = rng.uniform(0.3, 1.5) * 2 * np.pi * R / n
+    P = np.array([R + gap, 0.0, 0.0])
+    b = G.ring_points(P - R * u, nb, R, n)
+    return G.rings_to_tangle([a, b], (-0.05,) * 3, (0.05,) * 3, "open")
+
+
+def prepared(t, ref):
+    """tangents, normals and velocities as the reference has them before a pass"""
+    return ref.update_tangle(t, PARAMS, 0.0)
+
+
+def brute_candidates(t, rec_dist, rec_angle):
+    n = t.n
+    st = t.stat[:, 0]
+    ok = (st != -1) & (st != 1) & (st != 2)
+    lo = np.array(t.struct.box.bottom_left_back.p[:])
+    hi = np.array(t.struct.box.top_right_front.p[:])
+    L = hi - lo
+    per = np.array([t.struct.box.wall[2 * a] == 1 for a in range(3)])
+    tl = np.sqrt((t.tangents ** 2).sum(axis=1))
+    out = []
+    for k in range(n):
+        if not ok[k] or tl[k] < 0.5:
+            continue
+        for l in range(k + 1, n):
+            if not ok[l] or t.links[k, 0] == l or t.links[k, 1] == l or tl[l] < 0.5:
+                continue
+            d = t.pos[l] - t.pos[k]
+            w = t.pos[l].copy()
+            for a in range(3):
+                if per[a]:
+                    if d[a] > L[a] / 2:
+                        w[a] -= L[a]
+                    elif d[a] < -L[a] / 2:
+                        w[a] += L[a]
+            if np.sqrt(((t.pos[k] - w) ** 2).sum()) > rec_dist:
+                continue
+            c = (t.tangents[k] @ t.tangents[l]) / tl[k] / tl[l]
+            if c > np.cos(rec_angle):
+                continue
+            out.append((k, l))
+    return out
+
+
+def run_ours(ov, t, rec_dist):
+    lib = ov.load()
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+    out = t.copy()
+    out.set_images_from_library(lib)
+    n = lib.ov_reconnect_vortices(out.ptr(), 0.0, rec_dist, REC_ANGLE)
+    assert n >= 0, lib.ov_last_error_message()
+    return out, n
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_crossing_rings_match_reference(ov, seed):
+    ref = Ref()
+    t = prepared(crossing_rings(seed), ref)
+    rec_dist = 2 * 2 * np.pi * 1e-2 / 200
+    want, nw = ref.reconnect(t, PARAMS, 0.0, rec_dist, REC_ANGLE)
+    got, ng = run_ours(ov, t, rec_dist)
+    assert ng == nw
+    assert np.array_equal(got.links, want.links)
+    assert np.array_equal(got.recalc, want.recalc)
+    assert np.allclose(got.vels, want.vels, rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("boundary", ["open", "periodic-26"])
+def test_dense_tangle_matches_reference(ov, boundary):
+    ref = Ref()
+    D = 0.05
+    t = G.random_ring_tangle(17, 40, D, dl=D / 100, boundary=boundary)
+    t = prepared(t, ref)
+    rec_dist = 2.5 * D / 100
+    lib = ov.load()
+    pairs = np.zeros(2 * 100000, np.int32)
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+    t.set_images_from_library(lib)
+    m = lib.ov_reconnect_candidates(t.ptr(), rec_dist, REC_ANGLE, pairs.ctypes.data, 100000)
+    assert m >= 0, lib.ov_last_error_message()
+    cand = [tuple(p) for p in pairs[:2 * m].reshape(-1, 2)]
+    assert cand == brute_candidates(t, rec_dist, REC_ANGLE)
+    want, nw = ref.reconnect(t, PARAMS, 0.0, rec_dist, REC_ANGLE)
+    got, ng = run_ours(ov, t, rec_dist)
+    assert nw > 0, "the workload should reconnect somewhere"
+    assert ng == nw
+    assert np.array_equal(got.links, want.links)
+    assert np.array_equal(got.recalc, want.recalc)
+    assert np.allclose(got.vels, want.vels, rtol=1e-12, atol=0)
