@@ -440,6 +440,49 @@ def bench_adjoint(args, ov):
                     "cut-off crossed between the perturbed runs"}
 
 
+def bench_reconnect(args, ov, tangle, p):
+    """One vortex-vortex reconnection pass on the 1M-point tangle at the
+    0.087 rad angle cut-off: the GPU pair search and the whole pass (host
+    loop over the candidates with the approach test on the GPU).  rec_dist
+    is the tangle's point spacing DL (5e-4 cm): the reference's defaults pair
+    rec_dist = dl_min = 1e-3 cm with a remesh that keeps the spacing above
+    dl_min, so only nodes of different lines (or far along one line) are
+    candidates; a rec_dist of twice the spacing would also make every second
+    neighbour on the small rings a candidate.  The reference's O(N^2) pair
+    loop is timed on a 20k-point tangle of the same generator and scaled by
+    N^2."""
+    import time as _t
+    lib = ov.load()
+    rec_dist, rec_angle = DL, 0.087
+    ov.configure(p, ov.OV_PREC_FP64)
+    ht = tangle.copy()
+    ov.update_tangle(ht, 0.0)       # tangents of the current positions
+    lib.ov_reconnect_candidates(ht.ptr(), rec_dist, rec_angle, None, 0)   # warm-up
+    t0 = _t.perf_counter()
+    ncand = lib.ov_reconnect_candidates(ht.ptr(), rec_dist, rec_angle, None, 0)
+    t_search = _t.perf_counter() - t0
+    hc = ht.copy()
+    hc.set_images_from_library(lib)
+    t0 = _t.perf_counter()
+    nrec = lib.ov_reconnect_vortices(hc.ptr(), 0.0, rec_dist, rec_angle)
+    t_pass = _t.perf_counter() - t0
+    out = {"workload": f"{int(tangle.active.sum())} points, rec_dist={rec_dist}, rec_angle={rec_angle}",
+           "candidates": ncand, "reconnections": nrec, "gpu_search_s": t_search, "gpu_pass_s": t_pass}
+    from oracle.oracle import Ref, have_ref
+    if have_ref():
+        small, _ = make_tangle(20000, args.seed + 7)
+        ref = Ref(threads=os.cpu_count())
+        rs = ref.update_tangle(small, p, 0.0)
+        t0 = _t.perf_counter()
+        ref.reconnect(rs, p, 0.0, rec_dist, rec_angle)
+        t_ref = _t.perf_counter() - t0
+        ns, nb = int(small.active.sum()), int(tangle.active.sum())
+        out["reference_pass_s_20k"] = t_ref
+        out["reference_pass_s_estimate"] = t_ref * (nb / ns) ** 2
+        out["reference_note"] = "reference reconnect() on a 20k-point tangle (one thread: its loop is serial), scaled by N^2"
+    return out
+
+
 def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
@@ -575,11 +618,12 @@ def main():
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
 
-    direct = batch = adjoint = None
+    direct = batch = adjoint = reconnection = None
     if not args.no_extra:
         direct = bench_direct(args, ov, peak32.value, peak64.value)
         batch = bench_batch(args, ov, peak32.value)
         adjoint = bench_adjoint(args, ov)
+        reconnection = bench_reconnect(args, ov, tangle, p)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -623,6 +667,7 @@ def main():
             "direct_22k": direct,
             "batch_4096": batch,
             "adjoint_4096": adjoint,
+            "reconnection_1m": reconnection,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

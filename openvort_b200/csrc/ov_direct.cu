@@ -241,6 +241,9 @@ __global__ void k_add3(const double* a, const double* b, double* o, int n) {
 
 }  // namespace
 
+static bool ensure_segtab(ov_state_impl* s, const double* pos);
+bool ov_segment_table(ov_state_impl* s, const double* pos) { return ensure_segtab(s, pos); }
+
 static bool ensure_segtab(ov_state_impl* s, const double* pos) {
   if (!s->seg64.reserve(sizeof(double) * 6 * (size_t)s->n)) return false;
   if (!s->segid.reserve(sizeof(int) * (size_t)s->n)) return false;

@@ -158,6 +158,9 @@ bool ov_direct_points_scratch(cudaStream_t st, const OvParams& P, const double* 
                               const int2* links, const int2* status, int n, int npts,
                               const double* pts, const int* skip, double* seg, int* fwd,
                               double* part, double* out, double* img);
+// s->seg64 / s->segid: r1 and the wrapped r2 of every slot's forward
+// segment at positions pos, and the forward slot (-1: no segment)
+bool ov_segment_table(ov_state_impl* s, const double* pos);
 // out = a + b for n vectors of 3 doubles (device)
 bool ov_add3(cudaStream_t st, const double* a, const double* b, double* out, int n);
 

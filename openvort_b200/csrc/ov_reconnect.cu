@@ -137,9 +137,94 @@ __global__ void k_rec_scan(OvParams P, Grid g, const double* __restrict__ pos, c
       }
 }
 
+// ---------------------------------------------------------------- velocities
+// The nonlocal and image sums (update_velocity's loops, src/tangle.c:611-636)
+// at the two nodes of a candidate pair, spread over the whole GPU: block
+// (c, j) sums segments [c chunk, (c + 1) chunk) at image j of both nodes,
+// reduced in a fixed order in shared memory; k_pair_reduce then adds the
+// blocks in order.
+constexpr int kPV = 256;
+
+struct SegRef {
+  const double* r1r2;   // 6 doubles per slot: r1, wrapped r2 (k_segtab)
+  const int* fwd;
+};
+
+__global__ void __launch_bounds__(kPV) k_pair_vel(OvParams P, SegRef S, int n, const double* __restrict__ pos,
+                                                  int2 tk, int chunk, double* __restrict__ partial) {
+  __shared__ double red[kPV][6];
+  const int c = blockIdx.x, j = blockIdx.y, nch = gridDim.x;
+  d3 r[2];
+  int skip[2];
+  const int t2[2] = {tk.x, tk.y};
+#pragma unroll
+  for (int u = 0; u < 2; ++u) {
+    r[u] = ld3(pos, t2[u]);
+    skip[u] = -1;
+    if (j > 0) r[u] = image_point(P, j - 1, r[u]);
+    else skip[u] = t2[u];
+  }
+  double a[6] = {0, 0, 0, 0, 0, 0};
+  const int hi = min(n, (c + 1) * chunk);
+  for (int m = c * chunk + threadIdx.x; m < hi; m += kPV) {
+    const int fw = S.fwd[m];
+    if (fw < 0) continue;
+    const double* sg = S.r1r2 + 6 * (size_t)m;
+    const d3 r1 = mk3(sg[0], sg[1], sg[2]), r2 = mk3(sg[3], sg[4], sg[5]);
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (m == skip[u] || fw == skip[u]) continue;
+      const d3 v = seg_vel64(P.f4pi, r1, r2, r[u]);
+      a[3 * u] += v.x;
+      a[3 * u + 1] += v.y;
+      a[3 * u + 2] += v.z;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; ++q) red[threadIdx.x][q] = a[q];
+  __syncthreads();
+  for (int s = kPV / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s)
+      for (int q = 0; q < 6; ++q) red[threadIdx.x][q] += red[threadIdx.x + s][q];
+    __syncthreads();
+  }
+  if (threadIdx.x < 6) partial[((size_t)j * nch + c) * 6 + threadIdx.x] = red[0][threadIdx.x];
+}
+
+// v_nl and v_img of both nodes from the blocks' partial sums, in order;
+// mirror images reflect their velocity (src/tangle.c:633-634)
+__global__ void k_pair_reduce(OvParams P, const double* __restrict__ partial, int nch, int2 tk,
+                              double* v_nl, double* v_img) {
+  const int u = threadIdx.x;
+  if (u >= 2) return;
+  d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
+  for (int c = 0; c < nch; ++c) nl = nl + ld3(partial + (size_t)c * 6, u);
+  for (int j = 1; j <= P.n_img; ++j) {
+    d3 v = mk3(0, 0, 0);
+    for (int c = 0; c < nch; ++c) v = v + ld3(partial + ((size_t)j * nch + c) * 6, u);
+    const int face = P.img[j - 1][3];
+    if (face > -1) v = mirror_dir(v, face);
+    im = im + v;
+  }
+  const int k = u == 0 ? tk.x : tk.y;
+  st3(v_nl, k, nl);
+  st3(v_img, k, im);
+}
+
+// vels and vs of nodes k and l and the status flag, packed for one copy
+__global__ void k_pair_pack(const double* __restrict__ vels, const double* __restrict__ vs, int2 tk,
+                            const int* __restrict__ flag, double* out) {
+  const int i = threadIdx.x;
+  if (i < 12) {
+    const int node = i < 6 ? tk.x : tk.y, c = i % 3;
+    out[i] = (i % 6 < 3 ? vels : vs)[3 * (size_t)node + c];
+  }
+  if (i == 12) out[12] = (double)*flag;
+}
+
 struct RecState {
   ov_state_impl s;
-  DevBuf keys, keys2, ids, ids2, pairs, count, tmp, skip;
+  DevBuf keys, keys2, ids, ids2, pairs, count, tmp, skip, partial, pack;
 };
 
 RecState& rec_state() {
@@ -277,28 +362,59 @@ bool upload_for_pass(RecState& R, const tangle_state* t) {
   return true;
 }
 
-// update_velocity (src/tangle.c:583-684) of node k on the resident state
-// (direct sum: the reference passes no tree here), written back to the
-// tangle's vels[k] and vs[k]
-bool node_velocity(RecState& R, tangle_state* t, int k, double time) {
+// update_velocity (src/tangle.c:583-684) of nodes k and l on the resident
+// state (direct sum: the reference passes no tree here), written back to
+// the tangle's vels and vs
+bool pair_velocity(RecState& R, tangle_state* t, int k, int l, double time) {
   ov_state_impl* s = &R.s;
-  if (!R.skip.reserve(sizeof(int))) return false;
-  OV_TRY_CUDA(cudaMemcpyAsync(R.skip.p, &k, sizeof(int), cudaMemcpyHostToDevice, s->stream));
-  double* nl = s->v_nl.as<double>() + 3 * (size_t)k;
-  double* im = s->v_img.as<double>() + 3 * (size_t)k;
-  if (!s->P.lia_only &&
-      !ov_direct_points(s, s->pos.as<double>(), 1, s->pos.as<double>() + 3 * (size_t)k, R.skip.as<int>(),
-                        nullptr, 0, nl, im))
-    return false;
-  if (!ov_epilogue(s, time, s->pos.as<double>(), s->tan.as<double>(), s->nrm.as<double>(), s->v_nl.as<double>(),
-                   s->v_img.as<double>(), s->vels.as<double>(), s->vs.as<double>(), k, k + 1))
-    return false;
-  OV_TRY_CUDA(cudaMemcpyAsync(&t->vels[k], s->vels.as<double>() + 3 * (size_t)k, 24, cudaMemcpyDeviceToHost,
-                              s->stream));
-  OV_TRY_CUDA(cudaMemcpyAsync(&t->vs[k], s->vs.as<double>() + 3 * (size_t)k, 24, cudaMemcpyDeviceToHost,
-                              s->stream));
+  const int n = s->n;
+  const int2 tk = make_int2(k, l);
+  if (!s->P.lia_only) {
+    // segment table of the current links
+    if (!ov_segment_table(s, s->pos.as<double>())) return false;
+    const int nimg = s->P.n_img;
+    static int sms = 0;
+    if (!sms) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 1;
+    }
+    // about 8 blocks of 256 threads per SM: the FP64 sum is latency-bound
+    const int want = std::max(1, (8 * sms + nimg) / (nimg + 1));
+    const int chunk = std::max(kPV, (n + want - 1) / want);
+    const int nch = (n + chunk - 1) / chunk;
+    if (!R.partial.reserve(sizeof(double) * 6 * (size_t)nch * (nimg + 1))) return false;
+    k_pair_vel<<<dim3(nch, nimg + 1), kPV, 0, s->stream>>>(s->P, SegRef{s->seg64.as<double>(), s->segid.as<int>()},
+                                                           n, s->pos.as<double>(), tk, chunk, R.partial.as<double>());
+    OV_LAUNCHED();
+    k_pair_reduce<<<1, 32, 0, s->stream>>>(s->P, R.partial.as<double>(), nch, tk, s->v_nl.as<double>(),
+                                           s->v_img.as<double>());
+    OV_LAUNCHED();
+    OV_TRY_CUDA(cudaGetLastError());
+  }
+  int* flag = s->dflag.as<int>();
+  OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+  for (int u = 0; u < 2; ++u) {
+    const int m = u == 0 ? k : l;
+    if (!ov_launch_epilogue(s->stream, s->P, s->links.as<int2>(), s->status.as<int2>(), nullptr, time,
+                            s->pos.as<double>(), s->tan.as<double>(), s->nrm.as<double>(), s->v_nl.as<double>(),
+                            s->v_img.as<double>(), s->vels.as<double>(), s->vs.as<double>(), m, m + 1, flag))
+      return false;
+  }
+  if (!R.pack.reserve(sizeof(double) * 13)) return false;
+  k_pair_pack<<<1, 32, 0, s->stream>>>(s->vels.as<double>(), s->vs.as<double>(), tk, flag, R.pack.as<double>());
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  double h[13];
+  OV_TRY_CUDA(cudaMemcpyAsync(h, R.pack.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
   OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
-  return true;
+  for (int c = 0; c < 3; ++c) {
+    t->vels[k].p[c] = h[c];
+    t->vs[k].p[c] = h[3 + c];
+    t->vels[l].p[c] = h[6 + c];
+    t->vs[l].p[c] = h[9 + c];
+  }
+  return ov_flag_status((int)h[12], "update_velocity");
 }
 
 }  // namespace
@@ -341,7 +457,7 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     if (k == done_k || tangle->recalculate[k] || tangle->recalculate[l]) continue;
     if (tangle->connections[k].forward == l || tangle->connections[k].reverse == l) continue;
     // approach test on the current links (src/vortex_dynamics.c:266-277)
-    if (!node_velocity(R, tangle, k, t) || !node_velocity(R, tangle, l, t)) return -ov_last_error();
+    if (!pair_velocity(R, tangle, k, l, t)) return -ov_last_error();
     double w[3], dx[3], dv[3];
     h_pwrap(tangle, tangle->vnodes[k].p, tangle->vnodes[l].p, w);
     for (int c = 0; c < 3; ++c) {
