@@ -463,6 +463,7 @@ def bench_reconnect(args, ov, tangle, p):
     t_search = _t.perf_counter() - t0
     hc = ht.copy()
     hc.set_images_from_library(lib)
+    hc.recalc[:] = 0
     t0 = _t.perf_counter()
     nrec = lib.ov_reconnect_vortices(hc.ptr(), 0.0, rec_dist, rec_angle)
     t_pass = _t.perf_counter() - t0

@@ -427,10 +427,35 @@ int ov_adjoint_backward(ov_adjoint *a, const double *x_final_bar, double *x0_bar
  * do_reconnection (src/vortex_dynamics.c:317-364).  Its result is the
  * reference loop's: same links, flags, velocities written and count
  * (returned, or -OV_ERR_*).  Wall reconnections, small-loop removal and
- * domain cleanup stay with the reference's reconnect(). */
+ * domain cleanup stay with the reference's reconnect(), which zeroes
+ * tangle->recalculate before them: ov_reconnect_vortices reads the flags
+ * as it finds them, so a caller without the wall part zeroes them first. */
 int ov_reconnect_candidates(const struct tangle_state *tangle, double rec_dist, double rec_angle,
                             int *pairs, int max_pairs);
 int ov_reconnect_vortices(struct tangle_state *tangle, double t, double rec_dist, double rec_angle);
+
+/* ----- remesh and periodic wrap-around -----
+ * ov_remesh replaces remesh (src/tangle.c:824-873, include/tangle.h:155):
+ * the reference's slot-order loop that removes a node when a segment next
+ * to it is shorter than min_dist (merging it into that neighbour,
+ * remove_point) and the two together shorter than max_dist, and adds a
+ * node after a node whose forward segment is longer than max_dist
+ * (add_point), then enforce_boundaries if it added any.  Same nodes
+ * removed and added, same slots (search_next_free), same links; positions,
+ * tangents, normals and dxi as the reference's to rounding.  The tangle's
+ * dxi, tangents and normals must be current on entry (main.c computes them
+ * right before remesh) and are current on return.  New nodes take EMPTY
+ * slots; with none left, expand (the reference's expand_tangle) doubles
+ * the tangle, or without it the call fails with OV_ERR_INVALID after the
+ * changes made so far.  Returns the number of nodes removed plus added,
+ * or -OV_ERR_*.
+ * ov_enforce_boundaries replaces enforce_boundaries (src/tangle.c:796-819,
+ * include/tangle.h:118): every node outside the box through a periodic
+ * face moves by box lengths until it is inside.  Returns the number of
+ * nodes moved, or -OV_ERR_*. */
+typedef void (*ov_expand_fn)(struct tangle_state *tangle, size_t n);
+int ov_remesh(struct tangle_state *tangle, double min_dist, double max_dist, ov_expand_fn expand);
+int ov_enforce_boundaries(struct tangle_state *tangle);
 
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */

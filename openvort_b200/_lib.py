@@ -34,7 +34,7 @@ FUNCTIONS = [
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
     "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward",
-    "ov_reconnect_candidates", "ov_reconnect_vortices",
+    "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -148,6 +148,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "ov_reconnect_candidates": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p, C.c_int]),
         "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
+        "ov_remesh": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p]),
+        "ov_enforce_boundaries": (C.c_int, [T]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -3,85 +3,11 @@
 // hyperfriction, mutual friction, slip) and the RK4 stage arithmetic.
 // All FP64; each thread owns one node slot.  HBM-bound: ~150 B per node.
 #include "ov_internal.h"
+#include "ov_links.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-
-struct Links {
-  const int2* lk;   // (forward, reverse) per slot
-  const int2* st;   // (status, pin_wall) per slot
-};
-
-__device__ __forceinline__ bool pinned_any(int st) { return st == OV_PINNED || st == OV_PINNED_SLIP; }
-
-// Position `where` links away from node i (step_node, src/tangle.c:165-200).
-// Walking off a pinned end continues backwards on the mirror image of the
-// vortex.  Returns false on a broken link.
-__device__ bool step_node(const OvParams& P, const Links& L, const double* pos, int i,
-                          int where, d3& out) {
-  int faces[8];
-  int nf = 0;
-  int cur = i, w = where;
-  for (int it = 0; it < 16 && w != 0; ++it) {
-    int2 st = L.st[cur];
-    bool pin = pinned_any(st.x);
-    int2 lk = L.lk[cur];
-    int nx = w > 0 ? lk.x : lk.y;
-    if (nx >= 0) {
-      cur = nx;
-      w += w > 0 ? -1 : 1;
-    } else if (pin && nf < 8) {
-      faces[nf++] = st.y;
-      w = -w;
-    } else {
-      return false;
-    }
-  }
-  if (w != 0) return false;
-  d3 p = ld3(pos, cur);
-  for (int f = nf - 1; f >= 0; --f) {
-    int face = faces[f];
-    int c = face >> 1;
-    double wp = (face & 1) ? P.hi[c] : P.lo[c];
-    set_axis(p, c, 2.0 * wp - axis_of(p, c));
-  }
-  out = p;
-  return true;
-}
-
-// Arc length `dist` links away along the stored segment lengths
-// (arc_length, src/tangle.c:208-243); reverses at a pinned end.
-__device__ bool arc_length(const Links& L, const double* dxi, int k, int dist, double& out) {
-  double acc = 0;
-  int cur = k, d = dist;
-  for (int it = 0; it < 16 && d != 0; ++it) {
-    bool pin = pinned_any(L.st[cur].x);
-    int2 lk = L.lk[cur];
-    if (d > 0) {
-      if (lk.x < 0) {
-        if (!pin) return false;
-        d = -d;
-        continue;
-      }
-      acc += dxi[cur];
-      cur = lk.x;
-      --d;
-    } else {
-      if (lk.y < 0) {
-        if (!pin) return false;
-        d = -d;
-        continue;
-      }
-      acc += dxi[lk.y];
-      cur = lk.y;
-      ++d;
-    }
-  }
-  if (d != 0) return false;
-  out = acc;
-  return true;
-}
 
 // s' and s'' at x=0 from four points p_j at arc offsets x_j: weights are the
 // first and second derivatives at 0 of the Lagrange basis through {0, x_j}
@@ -103,10 +29,12 @@ __device__ void stencil4(const OvParams& P, d3 s0, const d3 p[4], const double x
   nrm = b;
 }
 
+// idx: the slots to compute (null: slots 0 .. n-1)
 __global__ void k_dxi(OvParams P, Links L, const double* __restrict__ pos, double* dxi,
-                      int n, int* flag) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+                      const int* __restrict__ idx, int n, int* flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = idx ? idx[i] : i;
   if (L.st[k].x == OV_EMPTY) return;
   d3 s0 = ld3(pos, k), s1;
   if (!step_node(P, L, pos, k, 1, s1)) { atomicOr(flag, 1); return; }
@@ -117,10 +45,11 @@ __global__ void k_dxi(OvParams P, Links L, const double* __restrict__ pos, doubl
 // pass 0: pinned and ordinary nodes; pass 1: nodes next to a pinned node,
 // which use their neighbours' tangents (src/tangle.c:366-430)
 __global__ void k_tangents(OvParams P, Links L, const double* __restrict__ pos,
-                           const double* __restrict__ dxi, double* tan, double* nrm, int n,
-                           int pass, int* flag) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+                           const double* __restrict__ dxi, double* tan, double* nrm,
+                           const int* __restrict__ idx, int n, int pass, int* flag) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = idx ? idx[i] : i;
   int2 st = L.st[k];
   if (st.x == OV_EMPTY) return;
   int2 lk = L.lk[k];
@@ -266,12 +195,19 @@ int blocks_for(int n) { return (n + kThreads - 1) / kThreads; }
 bool ov_launch_geometry(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
                         const double* pos, double* dxi, double* tan, double* nrm, int n, int* flag) {
   if (n <= 0) return true;
+  return ov_launch_geometry_list(st, P, links, status, pos, dxi, tan, nrm, nullptr, n, flag);
+}
+
+bool ov_launch_geometry_list(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                             const double* pos, double* dxi, double* tan, double* nrm, const int* idx, int n,
+                             int* flag) {
+  if (n <= 0) return true;
   Links L{links, status};
-  k_dxi<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, n, flag);
+  k_dxi<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, idx, n, flag);
   OV_LAUNCHED();
-  k_tangents<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, tan, nrm, n, 0, flag);
+  k_tangents<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, tan, nrm, idx, n, 0, flag);
   OV_LAUNCHED();
-  k_tangents<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, tan, nrm, n, 1, flag);
+  k_tangents<<<blocks_for(n), kThreads, 0, st>>>(P, L, pos, dxi, tan, nrm, idx, n, 1, flag);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   return true;

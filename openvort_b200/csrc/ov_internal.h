@@ -177,6 +177,11 @@ bool ov_state_reserve(ov_state_impl* s, int n);
 // non-finite velocity), read back later with ov_flag_status.
 bool ov_launch_geometry(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
                         const double* pos, double* dxi, double* tan, double* nrm, int n, int* flag);
+// the same for the slots idx[0 .. n-1] only (dxi of all of them first, then
+// the two tangent passes); the other slots' values are read as stored
+bool ov_launch_geometry_list(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                             const double* pos, double* dxi, double* tan, double* nrm, const int* idx, int n,
+                             int* flag);
 // epilogue at time t0 + *t_dev (t_dev may be null: time t0)
 bool ov_launch_epilogue(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
                         const double* t_dev, double t0, const double* pos, const double* tan,

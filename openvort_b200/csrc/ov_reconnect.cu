@@ -449,7 +449,9 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
   std::vector<int2> cand;
   if (!upload_for_pass(R, tangle) || !find_candidates(R, tangle, rec_dist, rec_angle, cand))
     return -ov_last_error();
-  for (int k = 0; k < tangle->N; ++k) tangle->recalculate[k] = 0;
+  // recalculate holds the sit-out flags on entry: the reference zeroes them
+  // at the top of reconnect (src/vortex_dynamics.c:148-149), before its wall
+  // part, whose reconnections the loop then leaves alone
   int nrecs = 0, done_k = -1;
   for (const int2& pr : cand) {
     const int k = pr.x, l = pr.y;

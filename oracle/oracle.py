@@ -214,6 +214,38 @@ class Ref:
         self.lib.refh_rk4_step(out.ptr(), C.c_double(time), C.c_double(dt))
         return out
 
+    def update_tangents_normals(self, t: HostTangle, p: Params) -> HostTangle:
+        """The reference's update_tangents_normals (src/tangle.c:704-727) on a copy."""
+        self.configure(p)
+        out = self._copy(t)
+        f = self.lib.update_tangents_normals
+        f.restype = None
+        f.argtypes = [C.c_void_p]
+        f(C.cast(out.ptr(), C.c_void_p))
+        return out
+
+    def remesh(self, t: HostTangle, p: Params, min_dist, max_dist) -> HostTangle:
+        """The reference's remesh (src/tangle.c:824-873) on a copy whose dxi,
+        tangents and normals are current; the copy keeps t's next_free."""
+        self.configure(p)
+        out = self._copy(t)
+        out.struct.next_free = t.struct.next_free
+        f = self.lib.remesh
+        f.restype = None
+        f.argtypes = [C.c_void_p, C.c_double, C.c_double]
+        f(C.cast(out.ptr(), C.c_void_p), min_dist, max_dist)
+        return out
+
+    def enforce_boundaries(self, t: HostTangle, p: Params) -> HostTangle:
+        """The reference's enforce_boundaries (src/tangle.c:796-819) on a copy."""
+        self.configure(p)
+        out = self._copy(t)
+        f = self.lib.enforce_boundaries
+        f.restype = None
+        f.argtypes = [C.c_void_p]
+        f(C.cast(out.ptr(), C.c_void_p))
+        return out
+
     def reconnect(self, t: HostTangle, p: Params, time, rec_dist, rec_angle):
         """The reference's reconnect (src/vortex_dynamics.c:140-313) on a copy
         whose tangents and normals are current; returns (copy, count)."""

@@ -86,6 +86,7 @@ def run_ours(ov, t, rec_dist):
     ov.configure(PARAMS, ov.OV_PREC_FP64)
     out = t.copy()
     out.set_images_from_library(lib)
+    out.recalc[:] = 0            # reconnect() zeroes them before its wall part
     n = lib.ov_reconnect_vortices(out.ptr(), 0.0, rec_dist, REC_ANGLE)
     assert n >= 0, lib.ov_last_error_message()
     return out, n
@@ -126,3 +127,34 @@ def test_dense_tangle_matches_reference(ov, boundary):
     assert np.array_equal(got.links, want.links)
     assert np.array_equal(got.recalc, want.recalc)
     assert np.allclose(got.vels, want.vels, rtol=1e-12, atol=0)
+
+
+def test_sit_out_flags_are_read_on_entry(ov):
+    """Nodes flagged before the loop (by the wall part of reconnect) sit the
+    pass out.  Pinned nodes sit it out the same way and change no other
+    node's velocity (src/tangle.c:586-590), so the reference's pass with the
+    flagged nodes pinned gives the same links and count."""
+    from openvort_b200.tangle import PINNED
+    ref = Ref()
+    t = prepared(crossing_rings(5), ref)   # two reconnections
+    rec_dist = 2 * 2 * np.pi * 1e-2 / 200
+    lib = ov.load()
+    base, n0 = run_ours(ov, t, rec_dist)
+    assert n0 > 0
+    out = t.copy()
+    out.set_images_from_library(lib)
+    out.recalc[:] = 1
+    assert lib.ov_reconnect_vortices(out.ptr(), 0.0, rec_dist, REC_ANGLE) == 0
+    assert np.array_equal(out.links, t.links)
+    flagged = np.nonzero(np.any(base.links != t.links, axis=1))[0][:3]
+    pinned = t.copy()
+    pinned.stat[flagged, 0] = PINNED
+    want, nw = ref.reconnect(pinned, PARAMS, 0.0, rec_dist, REC_ANGLE)
+    out = t.copy()
+    out.set_images_from_library(lib)
+    out.recalc[:] = 0
+    out.recalc[flagged] = 1
+    ng = lib.ov_reconnect_vortices(out.ptr(), 0.0, rec_dist, REC_ANGLE)
+    assert ng == nw
+    assert np.array_equal(out.links, want.links)
+    assert not np.array_equal(out.links, base.links)
