@@ -88,10 +88,11 @@ def params(theta):
                   vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}), vs=Flow("no flow"))
 
 
-def make_tangle(points, seed, alloc=np.empty):
+def make_tangle(points, seed, alloc=np.empty, empty_slots=0):
     from openvort_b200 import geometry as G
     n_rings = G.rings_for_points(points, D, dl=DL)
-    return G.random_ring_tangle(seed, n_rings, D, dl=DL, boundary="periodic-26", alloc=alloc), n_rings
+    return G.random_ring_tangle(seed, n_rings, D, dl=DL, boundary="periodic-26", alloc=alloc,
+                                empty_slots=empty_slots), n_rings
 
 
 def pinned_alloc():
@@ -484,6 +485,105 @@ def bench_reconnect(args, ov, tangle, p):
     return out
 
 
+def bench_remesh(args, ov):
+    """One remesh pass (ov_remesh, host tangle in and out) on a 1M-point
+    tangle with uneven resolution: 0.2% of the nodes pushed 30-80% of the
+    way to their forward neighbour, 500 pairs of nodes taken out;
+    min_dist = 0.6 dl, max_dist = 2.5 dl (the reference's defaults have a
+    1:5 ratio).  The reference's remesh, which recomputes every tangent after
+    each change, is timed on a 20k-point tangle of the same generator and
+    perturbation density and scaled by N^2."""
+    import time as _t
+    from openvort_b200 import geometry as G
+    lib = ov.load()
+    p = params(args.theta)
+    ov.configure(p, ov.OV_PREC_FP64)
+    lo, hi = 0.6 * DL, 2.5 * DL
+    t, _ = make_tangle(args.points, args.seed + 11, empty_slots=20000)
+    n = int(t.active.sum())
+    G.perturb_spacing(t, args.seed + 11, frac_move=0.002, n_gaps=n // 2000)
+    ov.update_tangents_normals(t)
+    warm = t.copy()
+    lib.ov_remesh(warm.ptr(), lo, hi, None)
+    run = t.copy()
+    t0 = _t.perf_counter()
+    changes = lib.ov_remesh(run.ptr(), lo, hi, None)
+    t_pass = _t.perf_counter() - t0
+    if changes < 0:
+        raise SystemExit(f"ov_remesh: {lib.ov_last_error_message().decode()}")
+    out = {"workload": f"{n} points, 0.2% of the nodes moved along the line, {n // 2000} node pairs "
+                       f"taken out, min_dist={lo:g}, max_dist={hi:g}",
+           "changes": changes, "gpu_pass_s": t_pass,
+           "path": "ov_remesh on a struct tangle_state in host memory (upload, GPU scan, host loop over "
+                   "the changes, GPU tangents near them, GPU enforce_boundaries, changed nodes back)"}
+    from oracle.oracle import Ref, have_ref
+    if have_ref():
+        small, _ = make_tangle(20000, args.seed + 11, empty_slots=400)
+        ns = int(small.active.sum())
+        G.perturb_spacing(small, args.seed + 11, frac_move=0.002, n_gaps=ns // 2000)
+        ref = Ref(threads=1)
+        rs = ref.update_tangents_normals(small, p)
+        t0 = _t.perf_counter()
+        ref.remesh(rs, p, lo, hi)
+        t_ref = _t.perf_counter() - t0
+        out["reference_pass_s_20k"] = t_ref
+        out["reference_pass_s_estimate"] = t_ref * (n / ns) ** 2
+        out["reference_note"] = ("reference remesh() on a 20k-point tangle (serial: each change runs "
+                                 "update_tangents_normals over all nodes), scaled by N^2")
+    return out
+
+
+def bench_frames(args, ov, tangle, p):
+    """Frames of the 1M-point state: the time until ov_state_save_frame
+    returns (device snapshot queued) and until the file is on disk, text
+    (the reference's format) and binary (with the time stamp); the
+    reference's save_tangle timed on a 200k-point tangle and scaled by N
+    (its loop is linear and serial)."""
+    import shutil
+    import time as _t
+    lib = ov.load()
+    ov.configure(p, ov.OV_PREC_FP64)
+    t = tangle.copy()
+    st = ov.DeviceState(t)
+    st.update_tangle(0.0)
+    n = int(t.active.sum())
+    out = {"workload": f"{n} points, frames of a device-resident state"}
+    tmp = tempfile.mkdtemp(prefix="ovframes")
+    try:
+        for name, binary in (("binary", True), ("text", False)):
+            path = os.path.join(tmp, f"frame.{name}")
+            st.save_frame(path, 0.0, binary=binary)      # warm-up (buffers)
+            st.wait_frames()
+            t0 = _t.perf_counter()
+            st.save_frame(path, 0.0, binary=binary)
+            t1 = _t.perf_counter()
+            st.wait_frames()
+            t2 = _t.perf_counter()
+            out[name] = {"call_s": t1 - t0, "written_s": t2 - t0, "bytes": os.path.getsize(path)}
+        from oracle.oracle import Ref, have_ref
+        if have_ref():
+            small, _ = make_tangle(200000, args.seed + 3)
+            st2 = ov.DeviceState(small)
+            st2.update_tangle(0.0)
+            st2.download()
+            st2.close()
+            ref = Ref()
+            f = ref.lib.save_tangle
+            f.restype = None
+            f.argtypes = [C.c_char_p, C.c_void_p]
+            t0 = _t.perf_counter()
+            f(os.path.join(tmp, "ref.dat").encode(), C.cast(small.ptr(), C.c_void_p))
+            t_ref = _t.perf_counter() - t0
+            ns = int(small.active.sum())
+            out["reference_text_s_200k"] = t_ref
+            out["reference_text_s_estimate"] = t_ref * n / ns
+    finally:
+        st.close()
+        shutil.rmtree(tmp, ignore_errors=True)
+    out["host_threads"] = os.cpu_count()
+    return out
+
+
 def main():
     args = parse()
     world, rank, local, dist = dist_setup(args)
@@ -619,12 +719,14 @@ def main():
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
 
-    direct = batch = adjoint = reconnection = None
+    direct = batch = adjoint = reconnection = remeshing = frames = None
     if not args.no_extra:
         direct = bench_direct(args, ov, peak32.value, peak64.value)
         batch = bench_batch(args, ov, peak32.value)
         adjoint = bench_adjoint(args, ov)
         reconnection = bench_reconnect(args, ov, tangle, p)
+        remeshing = bench_remesh(args, ov)
+        frames = bench_frames(args, ov, tangle, p)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -669,6 +771,8 @@ def main():
             "batch_4096": batch,
             "adjoint_4096": adjoint,
             "reconnection_1m": reconnection,
+            "remesh_1m": remeshing,
+            "frames_1m": frames,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

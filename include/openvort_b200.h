@@ -457,6 +457,45 @@ typedef void (*ov_expand_fn)(struct tangle_state *tangle, size_t n);
 int ov_remesh(struct tangle_state *tangle, double min_dist, double max_dist, ov_expand_fn expand);
 int ov_enforce_boundaries(struct tangle_state *tangle);
 
+/* ----- frames -----
+ * Text frames (OV_FRAME_TEXT) are the reference's save_tangle files
+ * (src/vortex_utils.c:308-345, include/vortex_utils.h), byte for byte:
+ * ov_save_tangle replaces save_tangle (without its "saving frame" line on
+ * stdout); the rows are formatted on all host cores.
+ * Binary frames (OV_FRAME_BINARY) add the simulation time, which text
+ * frames lack, and hold every slot as it is, little-endian:
+ *   struct ov_frame_header (128 bytes), then in slot order
+ *   vnodes, vels, tangents, normals   N x 3 doubles each
+ *   dxi                               N doubles
+ *   connections                       N x (forward, reverse) int32
+ *   status                            N x (status, pin_wall) int32
+ * (arrays the tangle does not have are written as zeros).
+ * ov_state_save_frame takes the frame from a device-resident state and
+ * returns at once: the state's arrays are copied on the device in its
+ * stream order, so later steps do not change the frame, and the file is
+ * written by a background thread.  A state's next frame waits for its
+ * previous one; ov_frame_wait waits for every pending write and returns
+ * the first failure.  ov_state_destroy waits for the state's frame; do not
+ * destroy a state while another thread is in ov_frame_wait.
+ * ov_load_frame reads a binary frame into a tangle of exactly the frame's
+ * slot count (ov_frame_info tells it), box and walls included. */
+enum { OV_FRAME_TEXT = 0, OV_FRAME_BINARY = 1 };
+typedef struct ov_frame_header {
+  char magic[8]; /* "OVFRAME" */
+  int32_t version; /* 1 */
+  int32_t n;       /* slots */
+  double time;     /* simulation time of the frame */
+  double box_lo[3], box_hi[3];
+  int32_t wall[6];
+  int32_t reserved[8];
+} ov_frame_header;
+int ov_save_tangle(const struct tangle_state *tangle, const char *filename);
+int ov_save_frame(const struct tangle_state *tangle, const char *filename, double time, int format);
+int ov_state_save_frame(ov_state *s, const char *filename, double time, int format);
+int ov_frame_wait(void);
+int ov_frame_info(const char *filename, int *n, double *time);
+int ov_load_frame(const char *filename, struct tangle_state *tangle, double *time);
+
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);

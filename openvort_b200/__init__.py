@@ -102,6 +102,15 @@ class DeviceState:
     def download(self, what: int = OV_FIELD_ALL):
         self._rc(self.lib.ov_state_download(self.h, self.t.ptr(), what))
 
+    def save_frame(self, path: str, time: float, binary: bool = True):
+        """Start writing a frame of the current state (ov_state_save_frame);
+        wait_frames() waits for the file."""
+        fmt = _lib.OV_FRAME_BINARY if binary else _lib.OV_FRAME_TEXT
+        self._rc(self.lib.ov_state_save_frame(self.h, str(path).encode(), time, fmt))
+
+    def wait_frames(self):
+        self._rc(self.lib.ov_frame_wait())
+
     def eval_points(self, pts: np.ndarray, skip=None, method: int = 0) -> np.ndarray:
         pts = np.ascontiguousarray(pts, dtype=np.float64)
         out = np.zeros_like(pts)

@@ -16,6 +16,7 @@ LIB_PATH = Path(__file__).resolve().parent / "libov_gpu.so"
 OV_OK, OV_ERR_NO_DEVICE, OV_ERR_CUDA, OV_ERR_INVALID = 0, 1, 2, 3
 OV_ERR_NONFINITE, OV_ERR_FLOW, OV_ERR_TREE_DEPTH, OV_ERR_TIMEOUT, OV_ERR_NOMEM = 4, 5, 6, 7, 8
 OV_PREC_FP64, OV_PREC_MIXED = 0, 1
+OV_FRAME_TEXT, OV_FRAME_BINARY = 0, 1
 OV_FIELD_POS, OV_FIELD_VELS, OV_FIELD_VS = 1, 2, 4
 OV_FIELD_TANGENTS, OV_FIELD_NORMALS, OV_FIELD_DXI, OV_FIELD_ALL = 8, 16, 32, 63
 
@@ -35,6 +36,8 @@ FUNCTIONS = [
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
     "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward",
     "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries",
+    "ov_save_tangle", "ov_save_frame", "ov_state_save_frame", "ov_frame_wait", "ov_frame_info",
+    "ov_load_frame",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -150,6 +153,12 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
         "ov_remesh": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p]),
         "ov_enforce_boundaries": (C.c_int, [T]),
+        "ov_save_tangle": (C.c_int, [T, C.c_char_p]),
+        "ov_save_frame": (C.c_int, [T, C.c_char_p, C.c_double, C.c_int]),
+        "ov_state_save_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_int]),
+        "ov_frame_wait": (C.c_int, []),
+        "ov_frame_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+        "ov_load_frame": (C.c_int, [C.c_char_p, T, C.POINTER(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -406,6 +406,7 @@ bool ov_state_reserve(ov_state_impl* s, int n) {
 }
 
 static void state_release(ov_state_impl* s) {
+  ov_frames_release(s);
   DevBuf* bufs[] = {&s->pos, &s->links, &s->status, &s->dxi, &s->tan, &s->nrm, &s->vels, &s->vs,
                     &s->pos0, &s->spos, &s->sdxi, &s->stan, &s->snrm, &s->svs, &s->k2, &s->k3,
                     &s->k4, &s->v_nl, &s->v_img, &s->img_part, &s->seg64, &s->segid, &s->dflag};
@@ -476,6 +477,7 @@ static bool upload_tangle(ov_state_impl* s, const tangle_state* t, bool need_flo
   }
   s->n_targets = nt;
   s->n_segments = ns;
+  for (int f = 0; f < 6; ++f) s->walls[f] = t->box.wall[f];
   if (n == 0) return true;
   return upload(s, t->vnodes, s->pos, 24 * n) && upload(s, t->connections, s->links, 8 * n) &&
          upload(s, t->status, s->status, 8 * n);
@@ -558,6 +560,8 @@ bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* 
 struct ov_state {
   ov_state_impl impl;
 };
+
+ov_state_impl* ov_state_impl_of(ov_state* s) { return &s->impl; }
 
 extern "C" {
 

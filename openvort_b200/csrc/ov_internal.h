@@ -120,7 +120,14 @@ struct ov_state_impl {
   long long launches_at_reset = 0;
   int n_targets = 0, n_segments = 0;
   cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
+  int walls[6] = {0, 0, 0, 0, 0, 0};   // box.wall of the uploaded tangle
+  void* frames = nullptr;              // frame snapshot buffers (ov_frames.cu)
 };
+
+// the implementation behind a public ov_state handle
+ov_state_impl* ov_state_impl_of(ov_state* s);
+// waits for and frees a state's frame buffers
+void ov_frames_release(ov_state_impl* s);
 
 // ---------------------------------------------------------------- launchers
 // geometry: dxi, tangents, normals of all slots (pos/links/status -> dxi,tan,nrm)

@@ -166,3 +166,43 @@ def wall_half_ring(n: int = 64, radius: float = 1e-2, box=0.05) -> HostTangle:
     pin[0] = pin[-1] = 4        # Z_L
     return HostTangle(pos, fwd, rev, status, pin, (-box, -box, 0.0), (box, box, 2 * box),
                       "wall-1-open")
+
+
+def perturb_spacing(t: HostTangle, seed: int, frac_move: float = 0.05, n_gaps: int = 6) -> HostTangle:
+    """Uneven resolution for remesh workloads, in place: a fraction of the
+    free nodes pushed 30-80% of the way to their forward neighbour (a short
+    segment and a long one), and n_gaps pairs of consecutive free nodes taken
+    out, their neighbours linked across the gap (one segment three spacings
+    long)."""
+    rng = np.random.default_rng(seed)
+    act = np.nonzero(t.active)[0]
+    free = act[t.stat[act, 0] == FREE]
+    periodic = t.boundary.startswith("periodic")
+    L = np.asarray(t.box_hi, dtype=np.float64) - np.asarray(t.box_lo, dtype=np.float64)
+    for k in rng.choice(free, size=max(1, int(frac_move * len(free))), replace=False):
+        f = t.links[k, 0]
+        if f < 0:
+            continue
+        d = t.pos[f] - t.pos[k]
+        if periodic:
+            d = d - L * np.round(d / L)
+        t.pos[k] += rng.uniform(0.3, 0.8) * d
+    done = set()
+    gaps = 0
+    for k in rng.choice(free, size=min(len(free), 4 * n_gaps), replace=False):
+        if gaps >= n_gaps:
+            break
+        a = int(k)
+        b = int(t.links[a, 0])
+        if b < 0 or t.stat[b, 0] != FREE:
+            continue
+        p, nx = int(t.links[a, 1]), int(t.links[b, 0])
+        if p < 0 or nx < 0 or nx == p or len({p, a, b, nx} & done):
+            continue
+        t.links[p, 0], t.links[nx, 1] = nx, p
+        for q in (a, b):
+            t.links[q] = -1
+            t.stat[q, 0] = EMPTY
+        done |= {p, a, b, nx}
+        gaps += 1
+    return t

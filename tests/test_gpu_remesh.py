@@ -47,43 +47,8 @@ def with_empty(t, extra):
     return out
 
 
-def min_image(t, d):
-    if t.boundary.startswith("periodic"):
-        L = np.asarray(t.box_hi) - np.asarray(t.box_lo)
-        d = d - L * np.round(d / L)
-    return d
-
-
 def perturb(t, seed, frac_move=0.05, n_gaps=6):
-    """Push nodes part of the way to their forward neighbour; take out pairs
-    of consecutive nodes (relinking around them)."""
-    rng = np.random.default_rng(seed)
-    act = np.nonzero(t.active)[0]
-    free = act[t.stat[act, 0] == 0]
-    for k in rng.choice(free, size=max(1, int(frac_move * len(free))), replace=False):
-        f = t.links[k, 0]
-        if f < 0:
-            continue
-        t.pos[k] += rng.uniform(0.3, 0.8) * min_image(t, t.pos[f] - t.pos[k])
-    done = set()
-    gaps = 0
-    for k in rng.choice(free, size=min(len(free), 4 * n_gaps), replace=False):
-        if gaps >= n_gaps:
-            break
-        a = int(k)
-        b = int(t.links[a, 0])
-        if b < 0 or t.stat[b, 0] != 0:
-            continue
-        p, nx = int(t.links[a, 1]), int(t.links[b, 0])
-        if p < 0 or nx < 0 or nx == p or len({p, a, b, nx} & done):
-            continue
-        t.links[p, 0], t.links[nx, 1] = nx, p
-        for q in (a, b):
-            t.links[q] = -1
-            t.stat[q, 0] = EMPTY
-        done |= {p, a, b, nx}
-        gaps += 1
-    return t
+    return G.perturb_spacing(t, seed, frac_move, n_gaps)
 
 
 def prepared(t, ref):
