@@ -191,6 +191,14 @@ extern double global_BH_grain;
 extern int global_hyperfriction;
 extern double global_max_curvature_scale;
 extern double global_hyperalpha;
+/* loop removal (include/vortex_constants.h:41,49-56) */
+extern int global_small_loop_cutoff;
+extern int global_eliminate_origin_loops;
+extern double global_eliminate_loops_origin_cutoff;
+extern int global_eliminate_zaxis_loops;
+extern double global_eliminate_loops_zaxis_cutoff;
+extern int global_eliminate_outer_loops;
+extern double global_eliminate_outer_loops_cutoff;
 
 /* ===================================================================== */
 /* Part 2: extensions (no reference counterpart)                          */
@@ -456,6 +464,17 @@ int ov_reconnect_vortices(struct tangle_state *tangle, double t, double rec_dist
 typedef void (*ov_expand_fn)(struct tangle_state *tangle, size_t n);
 int ov_remesh(struct tangle_state *tangle, double min_dist, double max_dist, ov_expand_fn expand);
 int ov_enforce_boundaries(struct tangle_state *tangle);
+
+/* ov_eliminate_small_loops replaces eliminate_small_loops
+ * (src/tangle.c:876-943, include/tangle.h:156): every closed loop or pinned
+ * line with fewer than loop_length + 1 nodes is emptied and unlinked, and
+ * before that, when global_eliminate_origin_loops / _zaxis_loops /
+ * _outer_loops are set, every loop lying wholly within the origin cut-off,
+ * within the z-axis cut-off or beyond the outer cut-off
+ * (src/tangle.c:945-1015).  The nodes removed and links left are the
+ * reference's; tangle->recalculate, which the reference uses as visit marks,
+ * is not written.  Returns the number of vortices removed, or -OV_ERR_*. */
+int ov_eliminate_small_loops(struct tangle_state *tangle, int loop_length);
 
 /* ----- frames -----
  * Text frames (OV_FRAME_TEXT) are the reference's save_tangle files

@@ -35,7 +35,7 @@ FUNCTIONS = [
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
     "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward",
-    "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries",
+    "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries", "ov_eliminate_small_loops",
     "ov_save_tangle", "ov_save_frame", "ov_state_save_frame", "ov_frame_wait", "ov_frame_info",
     "ov_load_frame",
 ]
@@ -46,6 +46,9 @@ DATA = [
     "global_alpha", "global_alpha_p", "global_dl_max", "global_num_threads",
     "global_use_mutual_friction", "global_use_BH", "global_BH_resolution", "global_BH_quadtree",
     "global_BH_grain", "global_hyperfriction", "global_max_curvature_scale", "global_hyperalpha",
+    "global_small_loop_cutoff", "global_eliminate_origin_loops", "global_eliminate_loops_origin_cutoff",
+    "global_eliminate_zaxis_loops", "global_eliminate_loops_zaxis_cutoff", "global_eliminate_outer_loops",
+    "global_eliminate_outer_loops_cutoff",
 ]
 
 
@@ -153,6 +156,7 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
         "ov_remesh": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p]),
         "ov_enforce_boundaries": (C.c_int, [T]),
+        "ov_eliminate_small_loops": (C.c_int, [T, C.c_int]),
         "ov_save_tangle": (C.c_int, [T, C.c_char_p]),
         "ov_save_frame": (C.c_int, [T, C.c_char_p, C.c_double, C.c_int]),
         "ov_state_save_frame": (C.c_int, [C.c_void_p, C.c_char_p, C.c_double, C.c_int]),

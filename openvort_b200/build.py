@@ -22,7 +22,7 @@ BUILD_DIR = PKG / "_build"
 LIB = PKG / "libov_gpu.so"
 SOURCES = ["ov_api.cu", "ov_geom.cu", "ov_direct.cu", "ov_tree.cu", "ov_walk.cu", "ov_peak.cu",
            "ov_noalloc.cu", "ov_batch.cu", "ov_adjoint.cu", "ov_reconnect.cu",
-           "ov_remesh.cu", "ov_frames.cu"]
+           "ov_remesh.cu", "ov_frames.cu", "ov_loops.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
                      "-I", str(ROOT / "include"), "-I", str(CSRC)]

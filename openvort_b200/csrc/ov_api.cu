@@ -41,6 +41,14 @@ double global_BH_grain = 1e-8;
 int global_hyperfriction = 1;
 double global_max_curvature_scale = 0.2;
 double global_hyperalpha = 0.5;
+// loop removal (src/vortex_constants.c:48,65-74)
+int global_small_loop_cutoff = 5;
+int global_eliminate_origin_loops = 0;
+double global_eliminate_loops_origin_cutoff = 3e-2;
+int global_eliminate_zaxis_loops = 0;
+double global_eliminate_loops_zaxis_cutoff = 2e-2;
+int global_eliminate_outer_loops = 0;
+double global_eliminate_outer_loops_cutoff = 1;
 struct v_conf_t vn_conf;
 struct v_conf_t vs_conf;
 struct v_conf_t vb_conf;

@@ -206,3 +206,39 @@ def perturb_spacing(t: HostTangle, seed: int, frac_move: float = 0.05, n_gaps: i
         done |= {p, a, b, nx}
         gaps += 1
     return t
+
+
+def relabel_slots(t: HostTangle, seed: int) -> HostTangle:
+    """The same tangle with its slots in a seeded random order (links
+    renumbered; vels, tangents, normals and dxi carried along)."""
+    rng = np.random.default_rng(seed)
+    n = len(t.pos)
+    perm = rng.permutation(n)               # old slot k -> new slot perm[k]
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+
+    def renum(x):
+        return np.where(x >= 0, perm[np.maximum(x, 0)], -1).astype(np.int32)
+
+    out = HostTangle(t.pos[inv], renum(t.links[inv, 0]), renum(t.links[inv, 1]), t.stat[inv, 0],
+                     t.stat[inv, 1], t.box_lo, t.box_hi, t.boundary)
+    for name in ("vels", "tangents", "normals", "dxi"):
+        getattr(out, name)[:] = getattr(t, name)[inv]
+    return out
+
+
+def join_tangles(parts: Sequence[HostTangle], box_lo, box_hi, boundary: str) -> HostTangle:
+    """Several tangles' slots side by side in one tangle."""
+    pos, fwd, rev, st, pin = [], [], [], [], []
+    off = 0
+    for t in parts:
+        n = len(t.pos)
+        pos.append(t.pos)
+        fwd.append(np.where(t.links[:, 0] >= 0, t.links[:, 0] + off, -1))
+        rev.append(np.where(t.links[:, 1] >= 0, t.links[:, 1] + off, -1))
+        st.append(t.stat[:, 0])
+        pin.append(t.stat[:, 1])
+        off += n
+    cat = np.concatenate
+    return HostTangle(cat(pos), cat(fwd).astype(np.int32), cat(rev).astype(np.int32), cat(st).astype(np.int32),
+                      cat(pin).astype(np.int32), box_lo, box_hi, boundary)

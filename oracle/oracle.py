@@ -236,6 +236,17 @@ class Ref:
         f(C.cast(out.ptr(), C.c_void_p), min_dist, max_dist)
         return out
 
+    def eliminate_small_loops(self, t: HostTangle, p: Params, loop_length: int) -> HostTangle:
+        """The reference's eliminate_small_loops (src/tangle.c:876-943) on a
+        copy, with the loop-removal globals as they are set in its library."""
+        self.configure(p)
+        out = self._copy(t)
+        f = self.lib.eliminate_small_loops
+        f.restype = None
+        f.argtypes = [C.c_void_p, C.c_int]
+        f(C.cast(out.ptr(), C.c_void_p), loop_length)
+        return out
+
     def enforce_boundaries(self, t: HostTangle, p: Params) -> HostTangle:
         """The reference's enforce_boundaries (src/tangle.c:796-819) on a copy."""
         self.configure(p)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from openvort_b200 import _lib, geometry as G
-from openvort_b200.tangle import EMPTY, HostTangle
+from openvort_b200.tangle import HostTangle
 from oracle.oracle import Ref, have_ref
 
 
@@ -39,21 +39,7 @@ def filled(t, seed):
 
 
 def relabel(t, seed):
-    """The same tangle with its slots in a random order."""
-    rng = np.random.default_rng(seed)
-    n = len(t.pos)
-    perm = rng.permutation(n)               # old slot k -> new slot perm[k]
-    inv = np.empty(n, np.int64)
-    inv[perm] = np.arange(n)
-
-    def m(x):
-        return np.where(x >= 0, perm[np.maximum(x, 0)], -1).astype(np.int32)
-
-    out = HostTangle(t.pos[inv], m(t.links[inv, 0]), m(t.links[inv, 1]), t.stat[inv, 0], t.stat[inv, 1],
-                     t.box_lo, t.box_hi, t.boundary)
-    for name in ("vels", "tangents", "normals", "dxi"):
-        getattr(out, name)[:] = getattr(t, name)[inv]
-    return out
+    return G.relabel_slots(t, seed)
 
 
 def cases():
