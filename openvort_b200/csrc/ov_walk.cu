@@ -22,6 +22,7 @@
 #include <float.h>
 
 #include "ov_internal.h"
+#include "ov_pair.cuh"
 
 namespace {
 
@@ -218,6 +219,9 @@ __device__ d3 warp_walk(const OvParams& P, const TreeView& T, d3 rp, bool live, 
 
 constexpr int kCombos = 27;
 constexpr int kPrimary = 13;
+// up to this many open images besides the target's own are decided one by
+// one; more take all 27 decisions at once (mac_exact)
+constexpr int kFewImages = 4;
 constexpr int kLevelSlots = 34;
 constexpr int kMultiWarps = 4;
 
@@ -321,11 +325,12 @@ __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 
   if (kMixed) nl = nl + mk3(fx, fy, fz);
 }
 
-// resident blocks per SM the register allocation must allow (measured at
-// 1M points: the walk is latency-bound, so more resident warps pay even
-// with a few registers spilled to L1)
+// resident blocks per SM the register allocation must allow, measured at
+// 1M points: mixed 71.3 / 74.4 / 72.8 / 80.3 ms for 4 / 5 / 6 / 3 blocks
+// (4 blocks leave 120 registers and no spills; the FP64 form spills less
+// at 5 than its extra warps cost)
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_MIXED
-#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 6
+#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 4
 #endif
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_FP64
 #define OV_WALK_MULTI_MIN_BLOCKS_FP64 5
@@ -383,8 +388,28 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
         unsigned pass;
         const double q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)),
                                     wrapped_sq(P, 2, r.z, cz));
-        if (q0 >= t0.x * (1.0 + 1e-10)) pass = m;
-        else pass = mac_exact(P, r, cx, cy, cz, t0.x);
+        if (q0 >= t0.x * (1.0 + 1e-10)) {
+          pass = m;
+        } else {
+          // q0 is the target's own decision in mac_exact's operations; the
+          // other images still open here are few below the top levels, so
+          // they are decided one by one unless there are many
+          pass = q0 >= t0.x ? (1u << kPrimary) : 0u;
+          unsigned rest = m & ~(1u << kPrimary);
+          if (__popc(rest) > kFewImages) {
+            pass |= mac_exact(P, r, cx, cy, cz, t0.x) & rest;
+          } else {
+            while (rest) {
+              const int c = __ffs(rest) - 1;
+              rest &= rest - 1;
+              const int ix = (c * 57) >> 9, rem = c - 9 * ix, iy = (rem * 11) >> 5, iz = rem - 3 * iy;
+              const double q = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, img_coord(r.x, P.L[0], ix), cx),
+                                                   wrapped_sq(P, 1, img_coord(r.y, P.L[1], iy), cy)),
+                                         wrapped_sq(P, 2, img_coord(r.z, P.L[2], iz), cz));
+              if (q >= t0.x) pass |= 1u << c;
+            }
+          }
+        }
         pass &= m;
         const unsigned fail = m & ~pass;
         if (kind == CELL_OPEN) open = fail;
@@ -393,65 +418,97 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
           n_far += __popc(pass);
           // expansion at every accepting image: R = r - L s - com, unwrapped
           if (kMixed) {
-            const float2 f0 = *reinterpret_cast<const float2*>(&cp->f_g[0]);
-            const float2 f1 = *reinterpret_cast<const float2*>(&cp->f_g[2]);
-            const float2 f2 = *reinterpret_cast<const float2*>(&cp->f_m12);
-            const float g0 = f0.x, g1 = f0.y, g2 = f1.x, m02 = f1.y, m12 = f2.x, m22 = f2.y;
+            const float2 q0f = *reinterpret_cast<const float2*>(&cp->f_g[0]);
+            const float2 q1f = *reinterpret_cast<const float2*>(&cp->f_g[2]);
+            const float2 q2f = *reinterpret_cast<const float2*>(&cp->f_m12);
+            const float g0 = q0f.x, g1 = q0f.y, g2 = q1f.x, m02 = q1f.y, m12 = q2f.x, m22 = q2f.y;
             const float m21 = __int_as_float(h.x);
-            // FP32 copies of the FP64-formed offsets r - L s - com per axis and shift
-            const float Fx[3] = {(float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
-                                 (float)__dsub_rn(r.x, cx),
-                                 (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx)};
-            const float Fy[3] = {(float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
-                                 (float)__dsub_rn(r.y, cy),
-                                 (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy)};
-            const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
-                                 (float)__dsub_rn(r.z, cz),
-                                 (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
-            // an accepting image has |R|^2 >= its wrapped squared distance >=
-            // thr, so a cell whose thr reaches the near radius needs no test
-            const bool test_near = t0.x < near2;
-            const float fnear2 = (float)near2;
-            float ax = 0, ay = 0, az = 0;
+            float ax, ay, az;
+            {
+              // FP32 copies of the FP64-formed offsets r - L s - com per axis and shift
+              const float Fx[3] = {(float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
+                                   (float)__dsub_rn(r.x, cx),
+                                   (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx)};
+              const float Fy[3] = {(float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
+                                   (float)__dsub_rn(r.y, cy),
+                                   (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy)};
+              const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
+                                   (float)__dsub_rn(r.z, cz),
+                                   (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+              // an accepting image has |R|^2 >= its wrapped squared distance >=
+              // thr, so a cell whose thr reaches the near radius needs no test
+              const bool test_near = t0.x < near2;
+              const float fnear2 = (float)near2;
+              // two (x, y) columns per packed FP32 pair: columns 2g and 2g + 1
+              // (the last group has column 8 only), their three z images
+              // evaluated side by side (independent chains), each image's
+              // terms summed where it accepts the cell
+              const f2 g0s = f2_splat(g0), g1s = f2_splat(g1), g2s = f2_splat(g2);
+              const f2 m02s = f2_splat(m02), m12s = f2_splat(m12), m22s = f2_splat(m22), m21s = f2_splat(m21);
+              f2 accx = f2_splat(0.f), accy = f2_splat(0.f), accz = f2_splat(0.f);
 #pragma unroll 1
-            for (int xy = 0; xy < 9; ++xy) {
-              const unsigned bits = (pass >> (3 * xy)) & 7u;
-              if (!bits) continue;
-              const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
-              const float X = sel3f(ix, Fx[0], Fx[1], Fx[2]);
-              const float Y = sel3f(iy, Fy[0], Fy[1], Fy[2]);
-              const float XY2 = fmaf(X, X, Y * Y);
-              // no z image of the column is nearer than its (x, y) distance
-              const bool col_near = test_near && XY2 < fnear2;
-              // the column's three z images evaluated side by side (independent
-              // chains), summed where they accept the cell
+              for (int grp = 0; grp < 5; ++grp) {
+                const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
+                const unsigned bits_a = (pass >> (3 * xa)) & 7u;
+                const unsigned bits_b = grp < 4 ? (pass >> (3 * xb)) & 7u : 0u;
+                if (!(bits_a | bits_b)) continue;
+                const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
+                const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
+                const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
+                const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
+                const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
+                const f2 nX = f2_pack(-Xa, -Xb), nY = f2_pack(-Ya, -Yb);
+                const f2 XY2 = f2_fma(X, X, Y * Y);
+                float xy2a, xy2b;
+                f2_unpack(XY2, xy2a, xy2b);
+                // no z image of a column is nearer than its (x, y) distance
+                const bool near_a = test_near && xy2a < fnear2, near_b = test_near && xy2b < fnear2;
 #pragma unroll
-              for (int iz = 0; iz < 3; ++iz) {
-                const float Z = Fz[iz];
-                const float R2 = fmaf(Z, Z, XY2);
-                const float inv = rsqrtf(R2);
-                const float inv2 = inv * inv;
-                const float i3 = inv2 * inv;
-                const float w = Z * inv2;
-                const float Gx = fmaf(m02, w, g0), Gy = fmaf(m12, w, g1), Gz = fmaf(m22, w, g2);
-                const float cxv = fmaf(Gy, Z, fmaf(-Gz, Y, m21));
-                const float cyv = fmaf(Gz, X, -Gx * Z);
-                const float czv = fmaf(Gx, Y, -Gy * X);
-                bool on = (bits >> iz) & 1u;
-                if (on && col_near && R2 < fnear2) {
-                  // near field: FP64 expansion from the FP64 offsets
-                  const d3 v = expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ix), cx),
-                                                      __dsub_rn(img_coord(r.y, P.L[1], iy), cy),
-                                                      __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
-                  nl = nl + v;
-                  on = false;
-                }
-                if (on) {
-                  ax = fmaf(cxv, i3, ax);
-                  ay = fmaf(cyv, i3, ay);
-                  az = fmaf(czv, i3, az);
+                for (int iz = 0; iz < 3; ++iz) {
+                  const float Z = Fz[iz];
+                  const f2 Zs = f2_splat(Z), nZ = f2_splat(-Z);
+                  const f2 R2 = f2_fma(Zs, Zs, XY2);
+                  const f2 inv = f2_rsqrt(R2);
+                  const f2 inv2 = inv * inv;
+                  const f2 i3 = inv2 * inv;
+                  const f2 w = Zs * inv2;
+                  const f2 Gx = f2_fma(m02s, w, g0s), Gy = f2_fma(m12s, w, g1s), Gz = f2_fma(m22s, w, g2s);
+                  const f2 cxv = f2_fma(Gy, Zs, f2_fma(Gz, nY, m21s));
+                  const f2 cyv = f2_fma(Gz, X, Gx * nZ);
+                  const f2 czv = f2_fma(Gx, Y, Gy * nX);
+                  bool on_a = (bits_a >> iz) & 1u, on_b = (bits_b >> iz) & 1u;
+                  if ((on_a && near_a) || (on_b && near_b)) {
+                    float r2a, r2b;
+                    f2_unpack(R2, r2a, r2b);
+                    // near field: FP64 expansion from the FP64 offsets
+                    if (on_a && near_a && r2a < fnear2) {
+                      nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixa), cx),
+                                                       __dsub_rn(img_coord(r.y, P.L[1], iya), cy),
+                                                       __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
+                      on_a = false;
+                    }
+                    if (on_b && near_b && r2b < fnear2) {
+                      nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixb), cx),
+                                                       __dsub_rn(img_coord(r.y, P.L[1], iyb), cy),
+                                                       __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
+                      on_b = false;
+                    }
+                  }
+                  float i3a, i3b;
+                  f2_unpack(i3, i3a, i3b);
+                  const f2 i3m = f2_pack(on_a ? i3a : 0.f, on_b ? i3b : 0.f);
+                  accx = f2_fma(cxv, i3m, accx);
+                  accy = f2_fma(cyv, i3m, accy);
+                  accz = f2_fma(czv, i3m, accz);
                 }
               }
+              float ax0, ax1, ay0, ay1, az0, az1;
+              f2_unpack(accx, ax0, ax1);
+              f2_unpack(accy, ay0, ay1);
+              f2_unpack(accz, az0, az1);
+              ax = ax0 + ax1;
+              ay = ay0 + ay1;
+              az = az0 + az1;
             }
             // the mixed form keeps one sum for the tangle and its images
             nl = nl + mk3(ax, ay, az);
