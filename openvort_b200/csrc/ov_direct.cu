@@ -117,7 +117,10 @@ constexpr int kPB = 128;            // threads per block
 constexpr int kPTgt = kPB * kTT;    // targets per block
 constexpr int kPSrc = 128;          // sources per shared-memory tile (kPSrc / 2 records)
 
-__global__ void __launch_bounds__(kPB, 5) k_direct_mixed_pairs(
+#ifndef OV_DIRECT_PAIRS_MIN_BLOCKS
+#define OV_DIRECT_PAIRS_MIN_BLOCKS 5
+#endif
+__global__ void __launch_bounds__(kPB, OV_DIRECT_PAIRS_MIN_BLOCKS) k_direct_mixed_pairs(
     OvParams P, SegTab S, int n_src, const double* __restrict__ pos, const int2* __restrict__ tstatus,
     const int* __restrict__ order, int n_t, int stride, double* __restrict__ part, int chunk) {
   __shared__ PairSrc<false> sh[kPSrc / 2];

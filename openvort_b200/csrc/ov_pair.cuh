@@ -82,7 +82,10 @@ __device__ __forceinline__ f2 f2_rcp(f2 a) {
 // nearer than the source's far radius, the pair is left to the caller's
 // FP64 path.
 
-constexpr int kTT = 2;   // targets per thread
+#ifndef OV_PAIR_TT
+#define OV_PAIR_TT 2
+#endif
+constexpr int kTT = OV_PAIR_TT;   // targets per thread
 constexpr float kColLo = 1e-8f * (1.0f - 2.5e-3f);
 constexpr float kColHi = 1e-8f * (1.0f + 2.5e-3f);
 

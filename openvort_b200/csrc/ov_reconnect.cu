@@ -350,7 +350,7 @@ bool find_candidates(RecState& R, const tangle_state* t, double rec_dist, double
 bool upload_for_pass(RecState& R, const tangle_state* t) {
   ov_state_impl* s = &R.s;
   if (!ov_upload_tangle(s, t)) return false;
-  if (!t->tangents || !t->normals) {
+  if (t->N > 0 && (!t->tangents || !t->normals)) {
     ov_set_error(OV_ERR_INVALID, "reconnection needs the tangle's tangents and normals");
     return false;
   }
@@ -441,7 +441,7 @@ int ov_reconnect_candidates(const struct tangle_state* tangle, double rec_dist, 
 
 int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist, double rec_angle) {
   ov_clear_error();
-  if (!tangle || rec_dist <= 0 || !tangle->recalculate || !tangle->vels || !tangle->vs) {
+  if (!tangle || rec_dist <= 0 || (tangle->N > 0 && (!tangle->recalculate || !tangle->vels || !tangle->vs))) {
     ov_set_error(OV_ERR_INVALID, "ov_reconnect_vortices: null tangle, arrays or rec_dist <= 0");
     return -OV_ERR_INVALID;
   }

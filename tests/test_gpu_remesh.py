@@ -169,3 +169,20 @@ def test_enforce_boundaries_matches_reference(ov, boundary):
     assert moved > 0, lib.ov_last_error_message()
     assert np.array_equal(got.pos[t.active], want.pos[t.active])
     assert moved == int(np.sum(np.any(want.pos[t.active] != t.pos[t.active], axis=1)))
+
+
+def test_empty_tangles(ov):
+    """N = 0 and a tangle of EMPTY slots only: nothing to do, no error."""
+    from openvort_b200.tangle import HostTangle
+    lib = ov.load()
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+    for n in (0, 5):
+        st = np.full(n, EMPTY, np.int32)
+        t = HostTangle(np.zeros((n, 3)), -np.ones(n, np.int32), -np.ones(n, np.int32), st, -np.ones(n, np.int32),
+                       (0, 0, 0), (D, D, D), "periodic-26")
+        assert lib.ov_remesh(t.ptr(), MIN, MAX, None) == 0, lib.ov_last_error_message()
+        assert lib.ov_enforce_boundaries(t.ptr()) == 0
+        assert lib.ov_eliminate_small_loops(t.ptr(), 5) == 0
+        assert lib.ov_reconnect_vortices(t.ptr(), 0.0, 1e-3, 0.087) == 0, lib.ov_last_error_message()
+        assert lib.ov_reconnect_candidates(t.ptr(), 1e-3, 0.087, None, 0) == 0
+        assert np.all(t.stat[:, 0] == EMPTY)
