@@ -58,8 +58,8 @@ HBM_PEAK, HBM_PEAK_SOURCE = _hbm_peak()
 FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
 # dram__bytes_read.sum + dram__bytes_write.sum of one mixed walk launch per
 # point, from the ncu launch list of this benchmark at 998,438 points
-# (323.1 MB per launch)
-WALK_DRAM_BYTES_PER_POINT = 323.6
+# (321.9 MB per launch)
+WALK_DRAM_BYTES_PER_POINT = 322.4
 
 
 def parse():
