@@ -720,7 +720,9 @@ def main():
                        "in pinned host memory"}
 
     direct = batch = adjoint = reconnection = remeshing = frames = None
-    if not args.no_extra:
+    # the single-GPU objects (and their CPU reference samples) belong to the
+    # 1-GPU line; a multi-GPU run measures the headline path only
+    if not args.no_extra and world == 1:
         direct = bench_direct(args, ov, peak32.value, peak64.value)
         batch = bench_batch(args, ov, peak32.value)
         adjoint = bench_adjoint(args, ov)
