@@ -222,6 +222,7 @@ constexpr int kPrimary = 13;
 // up to this many open images besides the target's own are decided one by
 // one; more take all 27 decisions at once (mac_exact)
 constexpr int kFewImages = 4;
+constexpr unsigned kAllImages = (1u << 27) - 1;
 constexpr int kLevelSlots = 34;
 constexpr int kMultiWarps = 4;
 
@@ -446,6 +447,50 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
               const f2 g0s = f2_splat(g0), g1s = f2_splat(g1), g2s = f2_splat(g2);
               const f2 m02s = f2_splat(m02), m12s = f2_splat(m12), m22s = f2_splat(m22), m21s = f2_splat(m21);
               f2 accx = f2_splat(0.f), accy = f2_splat(0.f), accz = f2_splat(0.f);
+              // All 27 images accept (the usual case: the wrapped opening test
+              // treats every image point like the target) and none is near:
+              // no per-image masks or near-field tests.  An image shifted
+              // along an axis has |R|^2 >= that axis offset squared (FP32
+              // rounding of sums of non-negative terms is monotonic), so when
+              // every shifted offset and the target's own |R|^2 reach the near
+              // radius, no image takes the FP64 path.
+              bool all_far = pass == kAllImages;
+              if (all_far && test_near) {
+                const float X = Fx[1], Y = Fy[1], Z = Fz[1];
+                all_far = fmaf(Z, Z, fmaf(X, X, Y * Y)) >= fnear2 && Fx[0] * Fx[0] >= fnear2 &&
+                          Fx[2] * Fx[2] >= fnear2 && Fy[0] * Fy[0] >= fnear2 && Fy[2] * Fy[2] >= fnear2 &&
+                          Fz[0] * Fz[0] >= fnear2 && Fz[2] * Fz[2] >= fnear2;
+              }
+              if (all_far) {
+#pragma unroll 1
+                for (int grp = 0; grp < 5; ++grp) {
+                  const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
+                  const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
+                  const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
+                  const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
+                  const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
+                  const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
+                  const f2 nX = f2_pack(-Xa, -Xb), nY = f2_pack(-Ya, -Yb);
+                  const f2 XY2 = f2_fma(X, X, Y * Y);
+                  // the last group holds column 8 twice: its second half is dropped
+                  const f2 keep = f2_pack(1.f, grp < 4 ? 1.f : 0.f);
+#pragma unroll
+                  for (int iz = 0; iz < 3; ++iz) {
+                    const float Z = Fz[iz];
+                    const f2 Zs = f2_splat(Z), nZ = f2_splat(-Z);
+                    const f2 R2 = f2_fma(Zs, Zs, XY2);
+                    const f2 inv = f2_rsqrt(R2);
+                    const f2 inv2 = inv * inv;
+                    f2 i3 = inv2 * inv;
+                    if (grp == 4) i3 = i3 * keep;
+                    const f2 w = Zs * inv2;
+                    const f2 Gx = f2_fma(m02s, w, g0s), Gy = f2_fma(m12s, w, g1s), Gz = f2_fma(m22s, w, g2s);
+                    accx = f2_fma(f2_fma(Gy, Zs, f2_fma(Gz, nY, m21s)), i3, accx);
+                    accy = f2_fma(f2_fma(Gz, X, Gx * nZ), i3, accy);
+                    accz = f2_fma(f2_fma(Gx, Y, Gy * nX), i3, accz);
+                  }
+                }
+              } else {
 #pragma unroll 1
               for (int grp = 0; grp < 5; ++grp) {
                 const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
@@ -501,6 +546,7 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
                   accy = f2_fma(cyv, i3m, accy);
                   accz = f2_fma(czv, i3m, accz);
                 }
+              }
               }
               float ax0, ax1, ay0, ay1, az0, az1;
               f2_unpack(accx, ax0, ax1);
