@@ -462,7 +462,8 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
                           Fz[0] * Fz[0] >= fnear2 && Fz[2] * Fz[2] >= fnear2;
               }
               if (all_far) {
-#pragma unroll 1
+                // unrolled: the column offsets are chosen at compile time
+#pragma unroll
                 for (int grp = 0; grp < 5; ++grp) {
                   const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
                   const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
