@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
             const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
             const double Rz[3] = {__dsub_rn(img_coord(r.z, P.L[2], 0), cz), __dsub_rn(r.z, cz),
                                   __dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
-#pragma unroll 1
+#pragma unroll
             for (int xy = 0; xy < 9; ++xy) {
               const unsigned bits = (pass >> (3 * xy)) & 7u;
               if (!bits) continue;
