@@ -57,9 +57,9 @@ def _hbm_peak():
 HBM_PEAK, HBM_PEAK_SOURCE = _hbm_peak()
 FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
 # dram__bytes_read.sum + dram__bytes_write.sum of one mixed walk launch per
-# point, from the ncu launch list of this benchmark at 998,438 points
-# (321.9 MB per launch)
-WALK_DRAM_BYTES_PER_POINT = 322.4
+# point, from the ncu launch list of this benchmark at 998,438 points (the
+# median of its 9 walk launches, 321.0 MB per launch)
+WALK_DRAM_BYTES_PER_POINT = 321.5
 
 
 def parse():
@@ -241,6 +241,39 @@ def run_reference_arm(args, world, rank):
 
 
 # ---------------------------------------------------------------- GPU side
+def bench_theta(args, ov, tangle, theta: float):
+    """The same 1M-point tangle at another opening angle: one RK4 step in
+    each form after one untimed step, and the mixed form's error against the
+    FP64 form over all nodes."""
+    n = int(tangle.active.sum())
+    p = params(theta)
+    out = {"theta": theta, "points": n}
+    vels = {}
+    for name, prec in (("mixed", ov.OV_PREC_MIXED), ("fp64", ov.OV_PREC_FP64)):
+        ov.configure(p, prec)
+        st = ov.DeviceState(tangle.copy())
+        st.run(0.0, args.dt, 1)
+        st.reset_stats()
+        st.run(args.dt, args.dt, 1)
+        rs = st.stats()
+        st.close()
+        s = ov.DeviceState(tangle.copy())
+        s.update_tangle(0.0)
+        s.download()
+        vels[name] = s.t.vels.copy()
+        s.close()
+        out[name] = {"ms_per_step": rs.last_run_ms, "value": n * 4 / (rs.last_run_ms / 1e3),
+                     "walk_ms": rs.bs_kernel_ms / max(1.0, rs.bs_launches),
+                     "cell_interactions_per_point": rs.cell_interactions / max(1.0, rs.bs_launches) / n}
+    act = tangle.active
+    out["mixed_over_fp64_speedup"] = out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    out["max_rel_err_mixed_vs_fp64"] = float(np.max(
+        np.linalg.norm(vels["mixed"][act] - vels["fp64"][act], axis=1) /
+        np.linalg.norm(vels["fp64"][act], axis=1)))
+    ov.configure(params(args.theta), ov.OV_PREC_MIXED)
+    return out
+
+
 def bench_direct(args, ov, peak32: float, peak64: float):
     """Direct all-pairs kernel on the 22.4k-point periodic tangle: 512 rings
     in a periodic cube D = 0.1 cm, radii U[0.02, 0.05] D, dl = D/200, 26
@@ -719,10 +752,11 @@ def main():
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
 
-    direct = batch = adjoint = reconnection = remeshing = frames = None
+    direct = batch = adjoint = reconnection = remeshing = frames = theta_alt = None
     # the single-GPU objects (and their CPU reference samples) belong to the
     # 1-GPU line; a multi-GPU run measures the headline path only
     if not args.no_extra and world == 1:
+        theta_alt = bench_theta(args, ov, tangle, 0.3 if args.theta != 0.3 else 0.5)
         direct = bench_direct(args, ov, peak32.value, peak64.value)
         batch = bench_batch(args, ov, peak32.value)
         adjoint = bench_adjoint(args, ov)
@@ -769,6 +803,7 @@ def main():
                                   "peak_source": HBM_PEAK_SOURCE + " copy bandwidth"}
                                  if traffic else None),
                          "tree_build_share_of_step": build_share},
+            "other_theta": theta_alt,
             "direct_22k": direct,
             "batch_4096": batch,
             "adjoint_4096": adjoint,

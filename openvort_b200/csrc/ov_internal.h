@@ -92,6 +92,8 @@ struct OvTree {
   DevBuf nodes32;       // per sorted node: r1 - cell-free origin (FP32 not used yet)
   DevBuf counters;      // device counters (interactions, cells visited)
   DevBuf scratch;
+  DevBuf scan_part;     // block sums of the exclusive scans
+  DevBuf mom_part;      // per-chunk partial moments of the largest cells
 };
 
 // ---------------------------------------------------------------- state

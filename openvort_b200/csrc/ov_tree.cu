@@ -24,6 +24,8 @@
 //     over each cell's own node range, as the reference does.
 #include <float.h>
 
+#include <algorithm>
+
 #include "ov_internal.h"
 
 namespace {
@@ -155,30 +157,72 @@ __global__ void k_rs_hist(const uint64_t* __restrict__ keys, int n, int shift, u
   hist[threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// exclusive scan of m unsigned values in one block of 1024 threads
-__global__ void k_scan_excl(unsigned* v, int m) {
-  __shared__ unsigned part[1024];
-  int per = (m + 1023) / 1024;
-  int b = threadIdx.x * per;
-  unsigned s = 0;
-  for (int i = 0; i < per; ++i)
-    if (b + i < m) s += v[b + i];
-  part[threadIdx.x] = s;
+// Exclusive scan of m unsigned values in three launches: the sum of each
+// 1024-value block, a scan of those sums, then every block's own scan plus
+// its offset.  Every access is one coalesced value per thread.
+constexpr int kScanThreads = 1024;
+
+// exclusive prefix of x over the block's threads (1024, 32 warps); the block
+// total in `total`.  sh holds 33 values.
+__device__ __forceinline__ unsigned block_excl_scan(unsigned x, unsigned* sh, unsigned& total) {
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned inc = x;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned y = __shfl_up_sync(FULL, inc, off);
+    if (lane >= off) inc += y;
+  }
+  if (lane == 31) sh[warp] = inc;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    unsigned x = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
-    __syncthreads();
-    part[threadIdx.x] += x;
-    __syncthreads();
-  }
-  unsigned run = part[threadIdx.x] - s;
-  for (int i = 0; i < per; ++i) {
-    if (b + i < m) {
-      unsigned x = v[b + i];
-      v[b + i] = run;
-      run += x;
+  if (warp == 0) {
+    const unsigned w = sh[lane];
+    unsigned wi = w;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned y = __shfl_up_sync(FULL, wi, off);
+      if (lane >= off) wi += y;
     }
+    sh[lane] = wi - w;
+    if (lane == 31) sh[32] = wi;
   }
+  __syncthreads();
+  total = sh[32];
+  const unsigned r = sh[warp] + inc - x;
+  __syncthreads();   // sh is free again on return
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(const unsigned* __restrict__ v, int m,
+                                                            unsigned* sums) {
+  __shared__ unsigned sh[33];
+  const int i = blockIdx.x * kScanThreads + threadIdx.x;
+  unsigned tot;
+  block_excl_scan(i < m ? v[i] : 0u, sh, tot);
+  if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+// one block: exclusive scan of nb block sums, 1024 at a time with a carry
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(unsigned* sums, int nb) {
+  __shared__ unsigned sh[33];
+  unsigned carry = 0;
+  for (int b0 = 0; b0 < nb; b0 += kScanThreads) {
+    const int i = b0 + threadIdx.x;
+    unsigned tot;
+    const unsigned e = block_excl_scan(i < nb ? sums[i] : 0u, sh, tot);
+    if (i < nb) sums[i] = carry + e;
+    carry += tot;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(unsigned* v, int m,
+                                                             const unsigned* __restrict__ sums) {
+  __shared__ unsigned sh[33];
+  const int i = blockIdx.x * kScanThreads + threadIdx.x;
+  const unsigned x = i < m ? v[i] : 0u;
+  unsigned tot;
+  const unsigned e = block_excl_scan(x, sh, tot);
+  if (i < m) v[i] = sums[blockIdx.x] + e;
 }
 
 __global__ void k_rs_scatter(const uint64_t* __restrict__ kin, const int* __restrict__ vin,
@@ -510,7 +554,7 @@ __global__ void k_moments_thread(const int* __restrict__ list, const int* __rest
   write_moments(cells + c, com, g, m21, m02, m12, m22, f4pi);
 }
 
-// same, one warp per cell (17..4096 nodes) or one block per cell (larger)
+// same, one warp per cell (17..4096 nodes)
 template <int kThreads>
 __device__ void moments_group(int c, Cell* cells, const int2* __restrict__ cell_range,
                               const double* __restrict__ nodes64,
@@ -582,13 +626,121 @@ __global__ void k_moments_warp(const int* __restrict__ list, const int* __restri
   moments_group<32>(list[w], cells, cell_range, nodes64, nodeids, f4pi, nullptr);
 }
 
-__global__ void k_moments_block(const int* __restrict__ list, const int* __restrict__ list_count,
-                                Cell* cells, const int2* __restrict__ cell_range,
-                                const double* __restrict__ nodes64,
-                                const int2* __restrict__ nodeids, double f4pi) {
-  __shared__ double sh[264];
-  if ((int)blockIdx.x >= *list_count) return;
-  moments_group<256>(list[blockIdx.x], cells, cell_range, nodes64, nodeids, f4pi, sh);
+// Cells of more than 4096 nodes: each cell's node range is cut into chunks of
+// `chunk` nodes, one block of kMomThreads per (cell, chunk), so the largest
+// cells (the root holds every node) spread over the GPU.  Partial sums per
+// chunk land in part[(j * max_chunks + k) * 10 + ...] (3 position sums, then
+// the 7 moment sums) and are added in chunk order, so the result does not
+// depend on scheduling.
+constexpr int kMomThreads = 256;
+constexpr int kMomChunk = 8192;      // smallest chunk
+constexpr int kMomMaxChunks = 64;    // chunks per cell at most
+
+// sum of v over the block's threads, in a fixed order; valid in thread 0
+template <int kN>
+__device__ __forceinline__ void block_sum(double (&v)[kN], double* sh) {
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < kN; ++q) {
+    double x = v[q];
+    for (int off = 16; off > 0; off >>= 1) x += __shfl_xor_sync(0xffffffffu, x, off);
+    v[q] = x;
+  }
+  if (ln == 0)
+    for (int q = 0; q < kN; ++q) sh[w * kN + q] = v[q];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 0; q < kN; ++q) {
+      double x = 0;
+      for (int ww = 0; ww < kMomThreads / 32; ++ww) x += sh[ww * kN + q];
+      v[q] = x;
+    }
+  }
+}
+
+// centre of mass of list cell j from its chunk position sums
+__device__ __forceinline__ d3 chunked_com(const double* __restrict__ part, int j, int max_chunks,
+                                          int count, int chunk) {
+  const int nch = (count + chunk - 1) / chunk;
+  double s[3] = {0, 0, 0};
+  for (int k = 0; k < nch; ++k) {
+    const double* pk = part + ((size_t)j * max_chunks + k) * 10;
+    s[0] += pk[0]; s[1] += pk[1]; s[2] += pk[2];
+  }
+  const double inv = 1.0 / count;
+  return mk3(s[0] * inv, s[1] * inv, s[2] * inv);
+}
+
+__global__ void __launch_bounds__(kMomThreads) k_moments_chunk_pos(
+    const int* __restrict__ list, const int2* __restrict__ cell_range,
+    const double* __restrict__ nodes64, int chunk, int max_chunks, double* part) {
+  __shared__ double sh[(kMomThreads / 32) * 3];
+  const int j = blockIdx.x, k = blockIdx.y;
+  const int2 rg = cell_range[list[j]];
+  const int lo = k * chunk;
+  if (lo >= rg.y) return;
+  const int hi = min(rg.y, lo + chunk);
+  double s[3] = {0, 0, 0};
+  for (int i = rg.x + lo + threadIdx.x; i < rg.x + hi; i += kMomThreads) {
+    const double* p = nodes64 + 6 * (size_t)i;
+    s[0] += p[0]; s[1] += p[1]; s[2] += p[2];
+  }
+  block_sum<3>(s, sh);
+  if (threadIdx.x == 0) {
+    double* o = part + ((size_t)j * max_chunks + k) * 10;
+    o[0] = s[0]; o[1] = s[1]; o[2] = s[2];
+  }
+}
+
+__global__ void __launch_bounds__(kMomThreads) k_moments_chunk_acc(
+    const int* __restrict__ list, const int2* __restrict__ cell_range,
+    const double* __restrict__ nodes64, const int2* __restrict__ nodeids, int chunk,
+    int max_chunks, double* part) {
+  __shared__ double sh[(kMomThreads / 32) * 7];
+  __shared__ double sh_com[3];
+  const int j = blockIdx.x, k = blockIdx.y;
+  const int2 rg = cell_range[list[j]];
+  const int lo = k * chunk;
+  if (lo >= rg.y) return;
+  const int hi = min(rg.y, lo + chunk);
+  if (threadIdx.x == 0) {
+    const d3 c = chunked_com(part, j, max_chunks, rg.y, chunk);
+    sh_com[0] = c.x; sh_com[1] = c.y; sh_com[2] = c.z;
+  }
+  __syncthreads();
+  const double cy = sh_com[1], cz = sh_com[2];
+  double a[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = rg.x + lo + threadIdx.x; i < rg.x + hi; i += kMomThreads) {
+    if (nodeids[i].y < 0) continue;
+    const double* p = nodes64 + 6 * (size_t)i;
+    const double dx = p[3] - p[0], dy = p[4] - p[1], dz = p[5] - p[2];
+    const double ly = p[1] - cy, lz = p[2] - cz;
+    a[0] += dx; a[1] += dy; a[2] += dz;
+    a[3] += dz * ly; a[4] += dx * lz; a[5] += dy * lz; a[6] += dz * lz;
+  }
+  block_sum<7>(a, sh);
+  if (threadIdx.x == 0) {
+    double* o = part + ((size_t)j * max_chunks + k) * 10 + 3;
+    for (int q = 0; q < 7; ++q) o[q] = a[q];
+  }
+}
+
+// one thread per list cell: chunk sums in chunk order into the cell record
+__global__ void k_moments_chunk_write(const int* __restrict__ list, const int* __restrict__ list_count,
+                                      Cell* cells, const int2* __restrict__ cell_range, int chunk,
+                                      int max_chunks, const double* __restrict__ part, double f4pi) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= *list_count) return;
+  const int c = list[j];
+  const int count = cell_range[c].y;
+  const d3 com = chunked_com(part, j, max_chunks, count, chunk);
+  const int nch = (count + chunk - 1) / chunk;
+  double a[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int k = 0; k < nch; ++k) {
+    const double* pk = part + ((size_t)j * max_chunks + k) * 10 + 3;
+    for (int q = 0; q < 7; ++q) a[q] += pk[q];
+  }
+  write_moments(cells + c, com, mk3(a[0], a[1], a[2]), a[3], a[4], a[5], a[6], f4pi);
 }
 
 // a tangle of one node: the root is that node's leaf
@@ -614,9 +766,24 @@ void ov_tree_release(OvTree* t) {
   DevBuf* bufs[] = {&t->keys, &t->keys_alt, &t->vals, &t->vals_alt, &t->stop, &t->hist,
                     &t->perm, &t->bnode, &t->cstart_cnt, &t->cbase, &t->cell_of, &t->cells,
                     &t->cell_lm, &t->cell_range, &t->nodes64, &t->nodeids, &t->nodes32, &t->counters,
-                    &t->scratch};
+                    &t->scratch, &t->scan_part, &t->mom_part};
   for (DevBuf* b : bufs) b->release();
   t->n_nodes = t->n_cells = t->built = 0;
+}
+
+// exclusive scan of v[0..m) in place (block sums in `part`)
+static bool scan_excl(unsigned* v, int m, DevBuf& part, cudaStream_t st) {
+  if (m <= 0) return true;
+  const int nb = (m + kScanThreads - 1) / kScanThreads;
+  if (!part.reserve(sizeof(unsigned) * (size_t)nb)) return false;
+  unsigned* sums = part.as<unsigned>();
+  k_scan_sums<<<nb, kScanThreads, 0, st>>>(v, m, sums);
+  OV_LAUNCHED();
+  k_scan_top<<<1, kScanThreads, 0, st>>>(sums, nb);
+  OV_LAUNCHED();
+  k_scan_apply<<<nb, kScanThreads, 0, st>>>(v, m, sums);
+  OV_LAUNCHED();
+  return ov_cuda_ok(cudaGetLastError(), "scan");
 }
 
 bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
@@ -672,8 +839,7 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     int shift = 8 * pass;
     k_rs_hist<<<nb_rs, kRsThreads, 0, st>>>(ka, n, shift, T->hist.as<unsigned>(), nb_rs);
     OV_LAUNCHED();
-    k_scan_excl<<<1, 1024, 0, st>>>(T->hist.as<unsigned>(), 256 * nb_rs);
-    OV_LAUNCHED();
+    if (!scan_excl(T->hist.as<unsigned>(), 256 * nb_rs, T->scan_part, st)) return false;
     k_rs_scatter<<<nb_rs, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, T->hist.as<unsigned>(), nb_rs);
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
@@ -742,8 +908,7 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     OV_TRY_CUDA(cudaMemsetAsync(base, 0, sizeof(unsigned) * (na + 1), st));
     k_classify<<<(nbin + 255) / 256, 256, 0, st>>>(bn, leaf_parent, term, na, info, base);
     OV_LAUNCHED();
-    k_scan_excl<<<1, 1024, 0, st>>>(base, na + 1);
-    OV_LAUNCHED();
+    if (!scan_excl(base, na + 1, T->scan_part, st)) return false;
     k_write_cells<<<(nbin + 255) / 256, 256, 0, st>>>(bn, leaf_parent, info, base, hi_sorted, klo,
                                                       T->nodes64.as<double>(), T->nodeids.as<int2>(),
                                                       s->P, na, cells, cell_lm, cell_range, lists,
@@ -769,8 +934,21 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
       OV_LAUNCHED();
     }
     if (lc[2] > 0) {
-      k_moments_block<<<lc[2], 256, 0, st>>>(lists + 4 * (size_t)na, list_counts + 2, cells, cell_range,
-                                             T->nodes64.as<double>(), T->nodeids.as<int2>(), f4);
+      // chunks of at least kMomChunk nodes, at most kMomMaxChunks per cell
+      const int chunk = std::max(kMomChunk, (na + kMomMaxChunks - 1) / kMomMaxChunks);
+      const int max_chunks = (na + chunk - 1) / chunk;
+      if (!T->mom_part.reserve(sizeof(double) * 10 * (size_t)lc[2] * max_chunks)) return false;
+      const int* blist = lists + 4 * (size_t)na;
+      double* part = T->mom_part.as<double>();
+      const dim3 grid(lc[2], max_chunks);
+      k_moments_chunk_pos<<<grid, kMomThreads, 0, st>>>(blist, cell_range, T->nodes64.as<double>(), chunk,
+                                                         max_chunks, part);
+      OV_LAUNCHED();
+      k_moments_chunk_acc<<<grid, kMomThreads, 0, st>>>(blist, cell_range, T->nodes64.as<double>(),
+                                                         T->nodeids.as<int2>(), chunk, max_chunks, part);
+      OV_LAUNCHED();
+      k_moments_chunk_write<<<(lc[2] + 127) / 128, 128, 0, st>>>(blist, list_counts + 2, cells, cell_range,
+                                                                  chunk, max_chunks, part, f4);
       OV_LAUNCHED();
     }
     OV_TRY_CUDA(cudaGetLastError());

@@ -270,3 +270,25 @@ def test_mixed_vs_fp64_large_bh(ov):
     a = gpu_update(ov, t, p, precision=0)
     b = gpu_update(ov, t, p, precision=1)
     assert rel_err(b.vels, a.vels, t.active) < TOL_MIXED
+
+
+def test_bh_tree_beyond_one_million_nodes(ov, oracle):
+    """A tree of ~1.09M nodes: the preorder scan over the cells spans more
+    than 1024 blocks of 1024 (its block sums are scanned in two rounds with a
+    carry) and the root cell's moments are summed in 64 chunks.  FP64
+    Barnes-Hut velocities at 48 points with the 26 periodic images, against
+    the oracle's recursive tree."""
+    from openvort_b200.tangle import IMAGE_TABLES
+    D, dl = 0.4, 0.4 / 800
+    t = G.random_ring_tangle(5, G.rings_for_points(1_100_000, D, dl=dl), D, dl=dl,
+                             boundary="periodic-26")
+    assert t.n > 1024 * 1024
+    p = Params(core_a=1e-8, dl_max=2 * dl, use_bh=1, bh_theta=0.5, bh_grain=1e-8)
+    ov.configure(p, 0)
+    st = ov.DeviceState(t.copy())
+    pts = np.random.default_rng(11).uniform(0, D, size=(48, 3))
+    shifts = [(0, 0, 0)] + [sh for sh, _ in IMAGE_TABLES["periodic-26"]]
+    allp = np.concatenate([pts - D * np.array(sh) for sh in shifts])
+    ref = oracle.bh_at(t, p, allp).reshape(len(shifts), len(pts), 3).sum(axis=0)
+    assert rel_err(st.eval_points(pts, method=1), ref) < TOL_V64
+    st.close()
