@@ -272,6 +272,29 @@ int ov_state_update_tangle(ov_state *s, double t);
 int ov_state_rk4_step(ov_state *s, double t, double dt);
 /* nsteps x (update_tangle + rk4_step), time advancing by dt */
 int ov_state_run(ov_state *s, double t0, double dt, int nsteps);
+/* ----- one tangle over several ranks (one process per GPU) -----
+ * Every rank holds the whole tangle and builds the same tree; rank r of W
+ * walks only the targets at key positions [r*c, (r+1)*c) of that tree,
+ * c = ceil(active nodes / W), so the Biot-Savart sums, nearly all the work
+ * of an evaluation, split W ways.  The sums are exchanged through xbuf, a
+ * device buffer of ov_state_shard_bytes(s, W) bytes (6 doubles per key
+ * position, rank r's block at r*c*6) that the caller all-gathers in place
+ * between begin and end (e.g. ncclAllGather with sendbuff = xbuf + r*c*6,
+ * recvbuff = xbuf, count c*6).  Every rank then finishes every node, so all
+ * ranks keep identical states and the results equal ov_state_run's bit for
+ * bit.  One RK4 step = stages 0..3, each begin / exchange / end:
+ *   stage 0: update_tangle at the positions (k1 into vels, vs)
+ *   stage q = 1..3: the q-th stage of rk4_step; stage 3 ends with the
+ *            combination that advances the positions
+ * begin returns once xbuf holds this rank's block; end reads all of xbuf.
+ * Needs the Barnes-Hut path (global_use_BH) unless global_LIA_only.  W = 1
+ * with xbuf NULL runs the same stages on one GPU.  No counterpart in the
+ * reference, which runs a tangle in one process. */
+int ov_state_shard(ov_state *s, int rank, int world, void *xbuf, size_t bytes);
+size_t ov_state_shard_bytes(ov_state *s, int world);
+int ov_state_shard_begin(ov_state *s, int stage, double t, double dt);
+int ov_state_shard_end(ov_state *s, int stage, double t, double dt);
+
 /* Biot-Savart velocity (nonlocal + images, no LIA/friction) at arbitrary
  * points from the state's current positions: method 0 = direct sum,
  * 1 = Barnes-Hut.  pts/out: host arrays of 3*npts doubles; skip: per-point

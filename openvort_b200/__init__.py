@@ -102,6 +102,20 @@ class DeviceState:
     def download(self, what: int = OV_FIELD_ALL):
         self._rc(self.lib.ov_state_download(self.h, self.t.ptr(), what))
 
+    # one tangle over several ranks (ov_state_shard*); openvort_b200.shard
+    # drives these with the exchange between begin and end
+    def shard_bytes(self, world: int) -> int:
+        return int(self.lib.ov_state_shard_bytes(self.h, world))
+
+    def shard(self, rank: int, world: int, xbuf_ptr: int | None, nbytes: int = 0):
+        self._rc(self.lib.ov_state_shard(self.h, rank, world, xbuf_ptr, nbytes))
+
+    def shard_begin(self, stage: int, time: float, dt: float):
+        self._rc(self.lib.ov_state_shard_begin(self.h, stage, time, dt))
+
+    def shard_end(self, stage: int, time: float, dt: float):
+        self._rc(self.lib.ov_state_shard_end(self.h, stage, time, dt))
+
     def save_frame(self, path: str, time: float, binary: bool = True):
         """Start writing a frame of the current state (ov_state_save_frame);
         wait_frames() waits for the file."""

@@ -29,7 +29,8 @@ FUNCTIONS = [
     "ov_get_precision", "ov_set_rk4_classic", "ov_get_rk4_classic", "ov_get_last_stats",
     "ov_state_create", "ov_state_destroy", "ov_state_upload", "ov_state_download",
     "ov_state_update_tangle", "ov_state_rk4_step", "ov_state_run", "ov_state_eval_points",
-    "ov_measure_fma_peak", "ov_state_get_stats", "ov_state_reset_stats",
+    "ov_measure_fma_peak", "ov_state_get_stats", "ov_state_reset_stats", "ov_state_shard",
+    "ov_state_shard_bytes", "ov_state_shard_begin", "ov_state_shard_end",
     "ov_set_mixed_near_factor", "ov_get_mixed_near_factor", "ov_direct_points_noalloc",
     "ov_batch_create", "ov_batch_destroy", "ov_batch_update", "ov_batch_run",
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
@@ -128,6 +129,10 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_state_eval_points": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
                                            C.c_void_p]),
         "ov_measure_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+        "ov_state_shard": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]),
+        "ov_state_shard_bytes": (C.c_size_t, [C.c_void_p, C.c_int]),
+        "ov_state_shard_begin": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
+        "ov_state_shard_end": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),
         "shifted": (Vec3d, [C.c_void_p, T, V]),
         "ov_state_get_stats": (C.c_int, [C.c_void_p, C.POINTER(RunStats)]),
         "ov_state_reset_stats": (None, [C.c_void_p]),

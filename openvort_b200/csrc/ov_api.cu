@@ -417,7 +417,8 @@ static void state_release(ov_state_impl* s) {
   ov_frames_release(s);
   DevBuf* bufs[] = {&s->pos, &s->links, &s->status, &s->dxi, &s->tan, &s->nrm, &s->vels, &s->vs,
                     &s->pos0, &s->spos, &s->sdxi, &s->stan, &s->snrm, &s->svs, &s->k2, &s->k3,
-                    &s->k4, &s->v_nl, &s->v_img, &s->img_part, &s->seg64, &s->segid, &s->dflag};
+                    &s->k4, &s->v_nl, &s->v_img, &s->img_part, &s->seg64, &s->segid, &s->dflag,
+                    &s->xown};
   for (DevBuf* b : bufs) b->release();
   ov_tree_release(&s->tree);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -463,7 +464,7 @@ static bool upload_tangle(ov_state_impl* s, const tangle_state* t, bool need_flo
   // interaction counts of the direct sum
   // and a check that every link and wall index the kernels follow is in
   // range, so a malformed tangle is an error instead of a stray device read
-  int nt = 0, ns = 0;
+  int nt = 0, ns = 0, na = 0;
   if (t->N > 0 && (!t->status || !t->connections)) {
     ov_set_error(OV_ERR_INVALID, "tangle without status or connection arrays");
     return false;
@@ -480,11 +481,13 @@ static bool upload_tangle(ov_state_impl* s, const tangle_state* t, bool need_flo
                    f, r, (int)t->status[k].pin_wall);
       return false;
     }
+    ++na;
     if (st != PINNED) ++nt;
     if (f >= 0) ++ns;
   }
   s->n_targets = nt;
   s->n_segments = ns;
+  s->n_active = na;
   for (int f = 0; f < 6; ++f) s->walls[f] = t->box.wall[f];
   if (n == 0) return true;
   return upload(s, t->vnodes, s->pos, 24 * n) && upload(s, t->connections, s->links, 8 * n) &&
@@ -517,10 +520,10 @@ bool ov_download_fields(ov_state_impl* s, tangle_state* t, int what) {
   return ok && sync(s);
 }
 
-bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* dxi,
-                   const double* tan, const double* nrm, double* vels, double* vs,
-                   OvTree* external_tree) {
-  (void)dxi;
+// The Biot-Savart sums of an evaluation into v_nl, v_img: the tree build and
+// walk (for the targets at key positions [k0, k0 + k_count) of the tree; all
+// of them when k_count < 0), or the direct sum.
+static bool bs_sums(ov_state_impl* s, const double* pos, OvTree* external_tree, int k0, int k_count) {
   tl_last_state = s;
   tl_stats = OvStatsAcc{0, 0, 0, 0, 0, 0, 0};
   cudaEventRecord(s->ev0, s->stream);
@@ -535,14 +538,21 @@ bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* 
         if (!ov_tree_build(s, pos, &s->tree)) return false;
         tree = &s->tree;
       }
-      if (!ov_tree_walk_nodes(s, tree, pos, tree == &s->tree, v_nl, v_img)) return false;
+      if (!ov_tree_walk_nodes(s, tree, pos, tree == &s->tree, v_nl, v_img, k0, k_count)) return false;
     } else {
       if (!ov_direct_nodes(s, pos, v_nl, v_img)) return false;
       // every target against every segment, per image (src/tangle.c:612-636)
       tl_stats.interactions = (double)s->n_targets * (double)s->n_segments * (1 + s->P.n_img);
     }
   }
-  if (!ov_epilogue(s, t, pos, tan, nrm, v_nl, v_img, vels, vs, 0, s->n)) return false;
+  return true;
+}
+
+// The epilogue of an evaluation over every node, and the state's counters.
+static bool finish_velocities(ov_state_impl* s, double t, const double* pos, const double* tan,
+                              const double* nrm, double* vels, double* vs) {
+  if (!ov_epilogue(s, t, pos, tan, nrm, s->v_nl.as<double>(), s->v_img.as<double>(), vels, vs, 0, s->n))
+    return false;
   // the epilogue synchronised the stream: fold this evaluation into the
   // state's counters (device times from the events around the tree build and
   // the Biot-Savart kernel)
@@ -560,6 +570,13 @@ bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* 
   s->acc_cells += tl_stats.cell_interactions;
   s->acc_warp_iter += tl_stats.warp_iterations;
   return true;
+}
+
+bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* dxi,
+                   const double* tan, const double* nrm, double* vels, double* vs,
+                   OvTree* external_tree) {
+  (void)dxi;
+  return bs_sums(s, pos, external_tree, 0, -1) && finish_velocities(s, t, pos, tan, nrm, vels, vs);
 }
 
 // ======================================================================
@@ -644,6 +661,116 @@ int ov_state_run(ov_state* st, double t0, double dt, int nsteps) {
   float ms = 0;
   cudaEventElapsedTime(&ms, s->ev_run0, s->ev_run1);
   s->last_run_ms = ms;
+  return OV_OK;
+}
+
+// ---------------------------------------------------------------- shards
+// Key positions per rank: c = ceil(active nodes / world); rank r holds
+// [r c, min((r + 1) c, active)).
+static int shard_chunk(const ov_state_impl* s, int world) {
+  return world > 0 ? (s->n_active + world - 1) / world : 0;
+}
+
+size_t ov_state_shard_bytes(ov_state* st, int world) {
+  if (!st || world < 1) return 0;
+  return sizeof(double) * 6 * (size_t)shard_chunk(&st->impl, world) * (size_t)world;
+}
+
+int ov_state_shard(ov_state* st, int rank, int world, void* xbuf, size_t bytes) {
+  ov_clear_error();
+  if (!st || world < 1 || rank < 0 || rank >= world) {
+    ov_set_error(OV_ERR_INVALID, "ov_state_shard: rank %d of %d", rank, world);
+    return tl_err;
+  }
+  ov_state_impl* s = &st->impl;
+  const size_t need = ov_state_shard_bytes(st, world);
+  if (!xbuf && world > 1) {
+    ov_set_error(OV_ERR_INVALID, "ov_state_shard: %d ranks need an exchange buffer", world);
+    return tl_err;
+  }
+  if (xbuf && (bytes < need || (reinterpret_cast<uintptr_t>(xbuf) & 7) != 0)) {
+    ov_set_error(OV_ERR_INVALID, "ov_state_shard: exchange buffer of %zu bytes at %p, need %zu, 8-aligned",
+                 bytes, xbuf, need);
+    return tl_err;
+  }
+  if (!xbuf) {
+    if (!s->xown.reserve(need > 0 ? need : 8)) return tl_err;
+    xbuf = s->xown.p;
+    bytes = s->xown.bytes;
+  }
+  s->shard_rank = rank;
+  s->shard_world = world;
+  s->xbuf = static_cast<double*>(xbuf);
+  s->xbytes = bytes;
+  return OV_OK;
+}
+
+// positions, geometry and outputs of stage q: 0 = update_tangle at the
+// positions, 1..3 = the stages of rk4_step2 (src/vortex_dynamics.c:76-92)
+struct ShardStage {
+  const double* pos;
+  double *dxi, *tan, *nrm, *vels, *vs;
+  double t;
+};
+
+static ShardStage shard_stage(ov_state_impl* s, int q, double t, double dt) {
+  if (q == 0)
+    return {s->pos.as<double>(), s->dxi.as<double>(), s->tan.as<double>(), s->nrm.as<double>(),
+            s->vels.as<double>(), s->vs.as<double>(), t};
+  double* ks[3] = {s->k2.as<double>(), s->k3.as<double>(), s->k4.as<double>()};
+  return {s->spos.as<double>(), s->sdxi.as<double>(), s->stan.as<double>(), s->snrm.as<double>(),
+          ks[q - 1], s->svs.as<double>(), q < 3 ? t + dt / 2 : t + dt};
+}
+
+static bool shard_ready(ov_state_impl* s, int q) {
+  if (q < 0 || q > 3) {
+    ov_set_error(OV_ERR_INVALID, "shard stage %d (0..3)", q);
+    return false;
+  }
+  if (!s->xbuf || s->xbytes < sizeof(double) * 6 * (size_t)shard_chunk(s, s->shard_world) * s->shard_world) {
+    ov_set_error(OV_ERR_INVALID, "no exchange buffer for %d active nodes: call ov_state_shard after the upload",
+                 s->n_active);
+    return false;
+  }
+  if (!s->P.lia_only && !s->P.use_bh) {
+    ov_set_error(OV_ERR_INVALID, "sharded evaluations need the Barnes-Hut path (global_use_BH)");
+    return false;
+  }
+  return true;
+}
+
+int ov_state_shard_begin(ov_state* st, int q, double t, double dt) {
+  ov_clear_error();
+  if (!st) { ov_set_error(OV_ERR_INVALID, "null state"); return tl_err; }
+  ov_state_impl* s = &st->impl;
+  s->P.precision = g_precision;
+  if (!shard_ready(s, q)) return tl_err;
+  if (q > 0 && !ov_rk4_stage_positions(s, q, dt, g_rk4_classic)) return tl_err;
+  const ShardStage g = shard_stage(s, q, t, dt);
+  if (!ov_geometry(s, g.pos, g.dxi, g.tan, g.nrm)) return tl_err;
+  const int c = shard_chunk(s, s->shard_world);
+  if (!bs_sums(s, g.pos, nullptr, s->shard_rank * c, c)) return tl_err;
+  s->shard_inter = tl_stats.interactions;
+  s->shard_cells = tl_stats.cell_interactions;
+  s->shard_warp_iter = tl_stats.warp_iterations;
+  if (!s->P.lia_only && !ov_shard_pack(s, s->shard_rank * c, c, s->xbuf, s->xbytes / sizeof(double)))
+    return tl_err;
+  // the caller's exchange reads xbuf from another stream
+  if (!sync(s)) return tl_err;
+  return OV_OK;
+}
+
+int ov_state_shard_end(ov_state* st, int q, double t, double dt) {
+  ov_clear_error();
+  if (!st) { ov_set_error(OV_ERR_INVALID, "null state"); return tl_err; }
+  ov_state_impl* s = &st->impl;
+  if (!shard_ready(s, q)) return tl_err;
+  const ShardStage g = shard_stage(s, q, t, dt);
+  if (!s->P.lia_only && !ov_shard_unpack(s, s->xbuf, s->xbytes / sizeof(double))) return tl_err;
+  tl_last_state = s;
+  tl_stats = OvStatsAcc{s->shard_inter, s->shard_cells, 0, 0, 0, 0, s->shard_warp_iter};
+  if (!finish_velocities(s, g.t, g.pos, g.tan, g.nrm, g.vels, g.vs)) return tl_err;
+  if (q == 3 && !(ov_rk4_combine(s, dt) && sync(s))) return tl_err;
   return OV_OK;
 }
 

@@ -295,32 +295,51 @@ bool ov_euler(ov_state_impl* s, double dt) {
   return true;
 }
 
+// Stage q = 1..3 positions of rk4_step2 (src/vortex_dynamics.c:76-92):
+// xs = x0 + h_q k_q, with k_1 = vels and k_2, k_3 the stage velocities; the
+// steps h are dt/2, dt/2 and, for the last stage, dt/2 like the reference
+// unless `classic` (dt).
+bool ov_rk4_stage_positions(ov_state_impl* s, int q, double dt, int classic) {
+  if (s->n == 0) return true;
+  const double h[3] = {dt / 2, dt / 2, classic ? dt : dt / 2};
+  double* x0 = s->pos.as<double>();
+  double* xs = s->spos.as<double>();
+  // EMPTY slots of the stage positions are never read, but keep them defined
+  if (q == 1)
+    OV_TRY_CUDA(cudaMemcpyAsync(xs, x0, sizeof(double) * 3 * s->n, cudaMemcpyDeviceToDevice, s->stream));
+  const double* prev = q == 1 ? s->vels.as<double>() : (q == 2 ? s->k2.as<double>() : s->k3.as<double>());
+  k_euler<<<blocks_for(s->n), kThreads, 0, s->stream>>>(s->status.as<int2>(), x0, prev, h[q - 1], xs,
+                                                         s->n);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+// x0 += dt/6 k1 + dt/3 k2 + dt/3 k3 + dt/6 k4 (src/vortex_dynamics.c:95-112)
+bool ov_rk4_combine(ov_state_impl* s, double dt) {
+  if (s->n == 0) return true;
+  k_rk4_combine<<<blocks_for(s->n), kThreads, 0, s->stream>>>(
+      s->status.as<int2>(), s->vels.as<double>(), s->k2.as<double>(), s->k3.as<double>(),
+      s->k4.as<double>(), dt, s->pos.as<double>(), s->n);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
 // rk4_step2 (src/vortex_dynamics.c:58-117) on the device state.  Stage 4
 // advances dt/2 like the reference unless `classic`.
 bool ov_rk4(ov_state_impl* s, double t, double dt, int classic) {
   if (s->n == 0) return true;
-  const int2* st = s->status.as<int2>();
-  double* x0 = s->pos.as<double>();
-  double* xs = s->spos.as<double>();
   double* ks[3] = {s->k2.as<double>(), s->k3.as<double>(), s->k4.as<double>()};
-  const double h[3] = {dt / 2, dt / 2, classic ? dt : dt / 2};
   const double ts[3] = {t + dt / 2, t + dt / 2, t + dt};
-  // EMPTY slots of the stage positions are never read, but keep them defined
-  OV_TRY_CUDA(cudaMemcpyAsync(xs, x0, sizeof(double) * 3 * s->n, cudaMemcpyDeviceToDevice, s->stream));
-  for (int q = 0; q < 3; ++q) {
-    const double* prev = q == 0 ? s->vels.as<double>() : ks[q - 1];
-    k_euler<<<blocks_for(s->n), kThreads, 0, s->stream>>>(st, x0, prev, h[q], xs, s->n);
-    OV_LAUNCHED();
-    OV_TRY_CUDA(cudaGetLastError());
+  const double* xs = s->spos.as<double>();
+  for (int q = 1; q <= 3; ++q) {
+    if (!ov_rk4_stage_positions(s, q, dt, classic)) return false;
     if (!ov_geometry(s, xs, s->sdxi.as<double>(), s->stan.as<double>(), s->snrm.as<double>()))
       return false;
-    if (!ov_velocities(s, ts[q], xs, s->sdxi.as<double>(), s->stan.as<double>(),
-                       s->snrm.as<double>(), ks[q], s->svs.as<double>(), nullptr))
+    if (!ov_velocities(s, ts[q - 1], xs, s->sdxi.as<double>(), s->stan.as<double>(),
+                       s->snrm.as<double>(), ks[q - 1], s->svs.as<double>(), nullptr))
       return false;
   }
-  k_rk4_combine<<<blocks_for(s->n), kThreads, 0, s->stream>>>(st, s->vels.as<double>(), ks[0], ks[1],
-                                                               ks[2], dt, x0, s->n);
-  OV_LAUNCHED();
-  OV_TRY_CUDA(cudaGetLastError());
-  return true;
+  return ov_rk4_combine(s, dt);
 }

@@ -124,6 +124,15 @@ struct ov_state_impl {
   cudaEvent_t ev_run0 = nullptr, ev_run1 = nullptr;
   int walls[6] = {0, 0, 0, 0, 0, 0};   // box.wall of the uploaded tangle
   void* frames = nullptr;              // frame snapshot buffers (ov_frames.cu)
+  // one tangle over several ranks (ov_state_shard): this rank's share of
+  // the targets, the exchange buffer, and the counters of the walk between
+  // ov_state_shard_begin and ov_state_shard_end
+  int n_active = 0;                    // non-EMPTY slots of the upload
+  int shard_rank = 0, shard_world = 1;
+  double* xbuf = nullptr;              // the caller's, or xown's when world is 1
+  size_t xbytes = 0;
+  DevBuf xown;
+  double shard_inter = 0, shard_cells = 0, shard_warp_iter = 0;
 };
 
 // the implementation behind a public ov_state handle
@@ -140,15 +149,25 @@ bool ov_velocities(ov_state_impl* s, double t, const double* pos, const double* 
                    OvTree* external_tree);
 // one RK4 step on the state's pos using the state's vels as k1
 bool ov_rk4(ov_state_impl* s, double t, double dt, int classic);
+// its pieces: stage q = 1..3 positions into spos, and the final combination
+bool ov_rk4_stage_positions(ov_state_impl* s, int q, double dt, int classic);
+bool ov_rk4_combine(ov_state_impl* s, double dt);
 bool ov_euler(ov_state_impl* s, double dt);
 
 // tree over the positions pos (slot-indexed); fills tree
 bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* tree);
 void ov_tree_release(OvTree* tree);
 // Barnes-Hut nonlocal + image sums for every active node -> v_nl, v_img
-// own_tree: the tree was built from `pos` (targets in its key order)
+// own_tree: the tree was built from `pos` (targets in its key order); then
+// only the targets at key positions [k0, k0 + k_count) are evaluated
+// (k_count < 0: all of them)
 bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* tree, const double* pos, bool own_tree,
-                        double* v_nl, double* v_img);
+                        double* v_nl, double* v_img, int k0 = 0, int k_count = -1);
+// sharded evaluations: v_nl, v_img of the targets at key positions
+// [k0, k0 + count) into xbuf (6 doubles per key position), and back from
+// xbuf for every active node; xcap: doubles in xbuf
+bool ov_shard_pack(ov_state_impl* s, int k0, int count, double* xbuf, size_t xcap);
+bool ov_shard_unpack(ov_state_impl* s, const double* xbuf, size_t xcap);
 // Barnes-Hut sums at arbitrary points (device arrays): out_nl = the tangle's
 // own sum (skip per point), out_img = the image sum (nullptr: no images)
 bool ov_tree_walk_points(ov_state_impl* s, OvTree* tree, int npts, const double* pts,

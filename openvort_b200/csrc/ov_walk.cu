@@ -21,6 +21,8 @@
 // test and near segments (|R| < 4 |ds|) in FP64.
 #include <float.h>
 
+#include <algorithm>
+
 #include "ov_internal.h"
 #include "ov_pair.cuh"
 
@@ -714,7 +716,7 @@ static bool read_counters(ov_state_impl* s, OvTree* t) {
 }
 
 bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own_tree,
-                        double* v_nl, double* v_img) {
+                        double* v_nl, double* v_img, int k0, int k_count) {
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(t->counters.as<char>() + 64);
   OV_TRY_CUDA(cudaMemsetAsync(ctr, 0, 24, s->stream));
   // a tree built from these positions: its key order; otherwise slot order
@@ -724,6 +726,18 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
     OV_TRY_CUDA(cudaMemsetAsync(v_nl, 0, sizeof(double) * 3 * s->n, s->stream));
     OV_TRY_CUDA(cudaMemsetAsync(v_img, 0, sizeof(double) * 3 * s->n, s->stream));
     return true;
+  }
+  // one rank's share: a contiguous range of the key order (each target's
+  // walk depends only on its own position, so the range changes no result)
+  if (own_tree && k_count >= 0) {
+    const int lo = std::min(std::max(k0, 0), n_t);
+    n_t = std::min(k_count, n_t - lo);
+    order += lo;
+    if (n_t <= 0) {
+      cudaEventRecord(s->ev1, s->stream);
+      cudaEventRecord(s->ev2, s->stream);
+      return read_counters(s, t);
+    }
   }
   TreeView tv = view_of(t);
   OvParams P = t->P;
@@ -810,4 +824,68 @@ bool ov_tree_walk_points(ov_state_impl* s, OvTree* t, int npts, const double* pt
   }
   OV_TRY_CUDA(cudaGetLastError());
   return read_counters(s, t);
+}
+
+// ---------------------------------------------------------------- shards
+namespace {
+
+__global__ void k_shard_pack(const int* __restrict__ perm, int k0, int count,
+                             const double* __restrict__ v_nl, const double* __restrict__ v_img,
+                             double* xbuf) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int k = perm[k0 + i];
+  double* o = xbuf + 6 * ((size_t)k0 + i);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    o[c] = v_nl[3 * (size_t)k + c];
+    o[3 + c] = v_img[3 * (size_t)k + c];
+  }
+}
+
+__global__ void k_shard_unpack(const int* __restrict__ perm, int n, const double* __restrict__ xbuf,
+                               double* v_nl, double* v_img) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int k = perm[i];
+  const double* x = xbuf + 6 * (size_t)i;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    v_nl[3 * (size_t)k + c] = x[c];
+    v_img[3 * (size_t)k + c] = x[3 + c];
+  }
+}
+
+// the exchange buffer holds 6 doubles per key position of the tree
+bool shard_fits(ov_state_impl* s, size_t xcap) {
+  if (6 * (size_t)s->tree.n_nodes <= xcap) return true;
+  ov_set_error(OV_ERR_INVALID, "tree of %d nodes beyond the exchange buffer (%zu doubles): call "
+               "ov_state_shard after the upload", s->tree.n_nodes, xcap);
+  return false;
+}
+
+}  // namespace
+
+bool ov_shard_pack(ov_state_impl* s, int k0, int count, double* xbuf, size_t xcap) {
+  if (!shard_fits(s, xcap)) return false;
+  const int n = s->tree.n_nodes;
+  k0 = std::min(std::max(k0, 0), n);
+  count = std::min(count, n - k0);
+  if (count <= 0) return true;
+  k_shard_pack<<<(count + 255) / 256, 256, 0, s->stream>>>(s->tree.perm.as<int>(), k0, count,
+                                                           s->v_nl.as<double>(), s->v_img.as<double>(), xbuf);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_shard_unpack(ov_state_impl* s, const double* xbuf, size_t xcap) {
+  if (!shard_fits(s, xcap)) return false;
+  const int n = s->tree.n_nodes;
+  if (n <= 0) return true;
+  k_shard_unpack<<<(n + 255) / 256, 256, 0, s->stream>>>(s->tree.perm.as<int>(), n, xbuf,
+                                                         s->v_nl.as<double>(), s->v_img.as<double>());
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
 }

@@ -1,7 +1,8 @@
-"""Multi-process rank plumbing (openvort_b200.dist) on CPU with gloo,
-world size 2: the timing collectives of multi-GPU runs, the per-rank seeds
-of the independent tangles, and a rank that never joins a collective
-ending the other's with an error (host-side failure detection)."""
+"""Multi-process rank plumbing (openvort_b200.dist, openvort_b200.shard) on
+CPU with gloo, world size 2: the timing collectives of multi-GPU runs, the
+per-rank seeds of the independent tangles, the in-place exchange of a
+tangle sharded over ranks, and a rank that never joins a collective ending
+the other's with an error (host-side failure detection)."""
 import os
 import socket
 
@@ -28,6 +29,15 @@ def _worker(rank, world, port, q, mode):
             mx = D.max_over_ranks(r, 1.5 + rank)
             sm = D.sum_over_ranks(r, 1.0 + rank)
             q.put((rank, mx, sm, D.rank_seed(2024, rank)))
+        elif mode == "exchange":
+            # sharded evaluations: each rank's block of the exchange buffer,
+            # all-gathered in place; the tail beyond world * block untouched
+            from openvort_b200.shard import exchange
+            block = 7
+            xbuf = torch.full((world * block + 3,), -1.0, dtype=torch.float64)
+            xbuf[rank * block:(rank + 1) * block] = torch.arange(block, dtype=torch.float64) + 100 * rank
+            exchange(xbuf, r, block)
+            q.put((rank, xbuf.tolist()))
         elif mode == "missing_rank":
             if rank == 1:
                 q.put((rank, "left"))           # leaves between steps, joins nothing
@@ -81,3 +91,14 @@ def test_rank_that_never_joins_ends_the_collective_with_an_error():
     out = _run("missing_rank")
     assert out[1][:2] == (1, "left")
     assert out[0][0] == 0 and out[0][1] == "error"
+
+
+def test_shard_exchange_world_2():
+    """The in-place all-gather between ov_state_shard_begin and _end: after
+    it every rank holds every rank's block, in rank order."""
+    out = _run("exchange")
+    block = 7
+    want = [float(i + 100 * r) for r in range(2) for i in range(block)] + [-1.0] * 3
+    assert [o[0] for o in out] == [0, 1]
+    for _, got in out:
+        assert got == want
