@@ -482,10 +482,16 @@ __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __rest
     }
     Lm = box_max(lo, hi);
     c.thr = mac_threshold(Lm, P.theta);
-    // moments are needed: file the cell by size for the moment kernels
+    // moments are needed: file the cell by size for the moment kernels,
+    // one atomic per class per warp (a list's order does not matter: each
+    // cell's moments depend on its own nodes only)
     int count = last - first + 1;
     int cls = count <= 16 ? 0 : (count <= 4096 ? 1 : 2);
-    int slot = atomicAdd(&list_counts[cls], 1);
+    const unsigned peers = __match_any_sync(__activemask(), cls);
+    const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+    int slot0 = 0;
+    if (lane == leader) slot0 = atomicAdd(&list_counts[cls], __popc(peers));
+    const int slot = __shfl_sync(peers, slot0, leader) + __popc(peers & ((1u << lane) - 1u));
     lists[cls * (size_t)(2 * n) + slot] = idx;
   }
   cells[idx] = c;
