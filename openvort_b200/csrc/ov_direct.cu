@@ -286,6 +286,14 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
   if (s->P.precision == OV_PREC_MIXED) {
     // spatially sorted order from the tree's key sort (timed as the build)
     if (!ov_tree_build(s, pos, &s->tree)) return false;
+    if (s->tree.n_nodes == 0) {
+      // every slot EMPTY: no targets and no segments
+      cudaEventRecord(s->ev1, s->stream);
+      cudaEventRecord(s->ev2, s->stream);
+      OV_TRY_CUDA(cudaMemsetAsync(v_nl, 0, sizeof(double) * 3 * s->n, s->stream));
+      OV_TRY_CUDA(cudaMemsetAsync(v_img, 0, sizeof(double) * 3 * s->n, s->stream));
+      return true;
+    }
     const int bx = (s->tree.n_nodes + kPTgt - 1) / kPTgt;
     const int chunk = source_chunk(s->tree.n_nodes, (long long)bx * (nimg + 1), kPSrc, &splits);
     if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;

@@ -292,3 +292,46 @@ def test_bh_tree_beyond_one_million_nodes(ov, oracle):
     ref = oracle.bh_at(t, p, allp).reshape(len(shifts), len(pts), 3).sum(axis=0)
     assert rel_err(st.eval_points(pts, method=1), ref) < TOL_V64
     st.close()
+
+
+def _ring5():
+    from openvort_b200.tangle import ring_points
+    r = ring_points(np.array([0.05, 0.05, 0.05]), (0.3, 0.2, 0.9), 0.004, 5)
+    return G.rings_to_tangle([r], (0, 0, 0), (0.1, 0.1, 0.1), "periodic-26", empty_slots=3)
+
+
+@pytest.mark.parametrize("use_bh", [0, 1])
+def test_smallest_loop_vs_oracle(ov, oracle, use_bh):
+    """A 5-node loop among EMPTY slots: the tree has a handful of cells and
+    every stencil reaches round the whole loop.  Velocities and one RK4 step
+    in FP64 against the oracle; the mixed form within its tolerance."""
+    t = _ring5()
+    p = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=1e-2, use_bh=use_bh,
+               bh_theta=0.5, vn=Flow("simple", {"external_v": (0.5, 0, 0)}))
+    ref = oracle.update_tangle(t, p)
+    g = gpu_update(ov, t, p)
+    assert rel_err(g.vels, ref.vels, t.active) < TOL_V64
+    ov.rk4_step(g, 0.0, 1e-6)
+    assert pos_err(g.pos, oracle.rk4_step(ref, p, 0.0, 1e-6).pos, t.active) < 1e-14
+    assert rel_err(gpu_update(ov, t, p, precision=1).vels, ref.vels, t.active) < TOL_MIXED
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("use_bh", [0, 1])
+def test_tangles_without_nodes(ov, use_bh, precision):
+    """N = 0, and slots that are all EMPTY: update_tangle, rk4_step and a
+    device-resident run have nothing to do and report no error."""
+    from openvort_b200.tangle import HostTangle
+    p = Params(core_a=1e-8, use_bh=use_bh, bh_theta=0.5)
+    for n in (0, 4):
+        t = HostTangle(np.zeros((n, 3)), -np.ones(n, np.int32), -np.ones(n, np.int32),
+                       np.full(n, -1, np.int32), -np.ones(n, np.int32), (0, 0, 0), (0.1, 0.1, 0.1),
+                       "periodic-26")
+        g = gpu_update(ov, t, p, precision=precision)
+        ov.rk4_step(g, 0.0, 1e-6)
+        assert np.array_equal(g.pos, t.pos)
+        st = ov.DeviceState(t.copy())
+        st.run(0.0, 1e-6, 2)
+        st.download()
+        assert np.array_equal(st.t.pos, t.pos)
+        st.close()

@@ -122,3 +122,20 @@ def test_shard_errors(ov, monkeypatch):
     with pytest.raises(ov.OVError):
         st.shard_begin(4, 0.0, DT)          # stages are 0..3
     st.close()
+
+
+def test_more_ranks_than_nodes(ov):
+    """8 ranks over a 5-node loop: ranks 5..7 own no targets, and every
+    rank still ends with the one-GPU state."""
+    from openvort_b200.tangle import ring_points
+    r = ring_points(np.array([0.05, 0.05, 0.05]), (0.3, 0.2, 0.9), 0.004, 5)
+    t = G.rings_to_tangle([r], (0, 0, 0), (0.1, 0.1, 0.1), "periodic-26", empty_slots=3)
+    p = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=1e-2, use_bh=1, bh_theta=0.5)
+    ov.configure(p, 0)
+    ref = ov.DeviceState(t.copy())
+    ref.run(0.0, DT, 2)
+    ref.download()
+    for st in run_ranks(ov, t, 8, 2):
+        assert np.array_equal(st.t.pos[t.active], ref.t.pos[t.active])
+        st.close()
+    ref.close()
