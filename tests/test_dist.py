@@ -38,6 +38,35 @@ def _worker(rank, world, port, q, mode):
             xbuf[rank * block:(rank + 1) * block] = torch.arange(block, dtype=torch.float64) + 100 * rank
             exchange(xbuf, r, block)
             q.put((rank, xbuf.tolist()))
+        elif mode == "sharded_run":
+            # ShardedRun's loop with a stand-in for the device state: at
+            # begin each rank writes its block, at end every block must be
+            # there; 4 stages per step, buffer sized by shard_bytes
+            from openvort_b200.shard import ShardedRun
+
+            class Stand:
+                n_active = 11
+                seen = []
+
+                def shard_bytes(self, world):
+                    return 48 * (-(-self.n_active // world)) * world
+
+                def shard(self, rank_, world_, ptr, nbytes):
+                    self.nbytes = nbytes
+
+                def shard_begin(self, q, t, dt):
+                    b = run.block
+                    run.xbuf[rank * b:(rank + 1) * b] = 1000 * q + 10 * rank + torch.arange(b)
+
+                def shard_end(self, q, t, dt):
+                    b = run.block
+                    want = torch.cat([1000 * q + 10 * rr + torch.arange(b) for rr in range(world)])
+                    self.seen.append((q, bool(torch.equal(run.xbuf[:world * b], want.double()))))
+
+            stand = Stand()
+            run = ShardedRun(stand, r)
+            run.run(0.0, 1e-6, 2)
+            q.put((rank, stand.nbytes, run.block, stand.seen))
         elif mode == "missing_rank":
             if rank == 1:
                 q.put((rank, "left"))           # leaves between steps, joins nothing
@@ -102,3 +131,12 @@ def test_shard_exchange_world_2():
     assert [o[0] for o in out] == [0, 1]
     for _, got in out:
         assert got == want
+
+
+def test_sharded_run_loop_world_2():
+    """ShardedRun.step: begin, the exchange, then end for each of the 4
+    stages; at every end all ranks' blocks are in the buffer."""
+    out = _run("sharded_run")
+    for rank, nbytes, block, seen in out:
+        assert nbytes == 48 * 6 * 2 and block == 6 * 6
+        assert seen == [(q, True) for _ in range(2) for q in range(4)]
