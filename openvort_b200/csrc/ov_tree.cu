@@ -560,15 +560,15 @@ __global__ void k_moments_thread(const int* __restrict__ list, const int* __rest
   write_moments(cells + c, com, g, m21, m02, m12, m22, f4pi);
 }
 
-// same, one warp per cell (17..4096 nodes)
-template <int kThreads>
-__device__ void moments_group(int c, Cell* cells, const int2* __restrict__ cell_range,
-                              const double* __restrict__ nodes64,
-                              const int2* __restrict__ nodeids, double f4pi, double* sh) {
-  const int tid = kThreads == 32 ? (threadIdx.x & 31) : threadIdx.x;
+// same, one warp per cell (17..4096 nodes): lane-strided sums, then a
+// butterfly over the warp
+__device__ void moments_warp(int c, Cell* cells, const int2* __restrict__ cell_range,
+                             const double* __restrict__ nodes64,
+                             const int2* __restrict__ nodeids, double f4pi) {
+  const int tid = threadIdx.x & 31;
   const int start = cell_range[c].x, count = cell_range[c].y;
   double s[3] = {0, 0, 0};
-  for (int i = start + tid; i < start + count; i += kThreads) {
+  for (int i = start + tid; i < start + count; i += 32) {
     const double* p = nodes64 + 6 * (size_t)i;
     s[0] += p[0]; s[1] += p[1]; s[2] += p[2];
   }
@@ -577,25 +577,10 @@ __device__ void moments_group(int c, Cell* cells, const int2* __restrict__ cell_
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     s[q] = v;
   }
-  if (kThreads > 32) {
-    int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    if (ln == 0) for (int q = 0; q < 3; ++q) sh[w * 8 + q] = s[q];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int q = 0; q < 3; ++q) {
-        double v = 0;
-        for (int ww = 0; ww < kThreads / 32; ++ww) v += sh[ww * 8 + q];
-        sh[256 + q] = v;
-      }
-    }
-    __syncthreads();
-    for (int q = 0; q < 3; ++q) s[q] = sh[256 + q];
-    __syncthreads();
-  }
   double inv = 1.0 / count;
   d3 com = mk3(s[0] * inv, s[1] * inv, s[2] * inv);
   double a[7] = {0, 0, 0, 0, 0, 0, 0};
-  for (int i = start + tid; i < start + count; i += kThreads) {
+  for (int i = start + tid; i < start + count; i += 32) {
     if (nodeids[i].y < 0) continue;
     const double* p = nodes64 + 6 * (size_t)i;
     double dx = p[3] - p[0], dy = p[4] - p[1], dz = p[5] - p[2];
@@ -608,18 +593,6 @@ __device__ void moments_group(int c, Cell* cells, const int2* __restrict__ cell_
     for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
     a[q] = v;
   }
-  if (kThreads > 32) {
-    int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-    if (ln == 0) for (int q = 0; q < 7; ++q) sh[w * 8 + q] = a[q];
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int q = 0; q < 7; ++q) {
-        double v = 0;
-        for (int ww = 0; ww < kThreads / 32; ++ww) v += sh[ww * 8 + q];
-        a[q] = v;
-      }
-    }
-  }
   if (tid == 0) write_moments(cells + c, com, mk3(a[0], a[1], a[2]), a[3], a[4], a[5], a[6], f4pi);
 }
 
@@ -629,7 +602,7 @@ __global__ void k_moments_warp(const int* __restrict__ list, const int* __restri
                                const int2* __restrict__ nodeids, double f4pi) {
   int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= *list_count) return;
-  moments_group<32>(list[w], cells, cell_range, nodes64, nodeids, f4pi, nullptr);
+  moments_warp(list[w], cells, cell_range, nodes64, nodeids, f4pi);
 }
 
 // Cells of more than 4096 nodes: each cell's node range is cut into chunks of
