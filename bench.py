@@ -709,6 +709,9 @@ def main():
     from openvort_b200.dist import rank_seed
     tangle, n_rings = make_tangle(args.points, rank_seed(args.seed, rank))
     n = int(tangle.active.sum())
+    # every rank its own tangle: the job's points are the sum over ranks
+    from openvort_b200.dist import sum_over_ranks
+    n_job = int(round(sum_over_ranks(dist, float(n))))
 
     # ---------------- device-resident timing, mixed precision
     ov.configure(p, ov.OV_PREC_MIXED)
@@ -725,7 +728,7 @@ def main():
     rs = st.stats()
     ms_run = max_over_ranks(dist, rs.last_run_ms)
     ms_step = ms_run / args.steps
-    value = world * n * 4 * args.steps / (ms_run / 1e3)
+    value = n_job * 4 * args.steps / (ms_run / 1e3)
     # roofline of the Barnes-Hut walk: algorithmic flops per launch / device
     # time per launch (CUDA events around each walk launch on its stream)
     flops = rs.interactions * FLOPS_P2P + rs.cell_interactions * FLOPS_CELL
@@ -749,7 +752,7 @@ def main():
     barrier(dist)
     rs64 = st64.stats()
     ms64 = max_over_ranks(dist, rs64.last_run_ms) / args.fp64_steps
-    value64 = world * n * 4 / (ms64 / 1e3)
+    value64 = n_job * 4 / (ms64 / 1e3)
     peak64 = C.c_double(0)
     lib.ov_measure_fma_peak(1, C.byref(peak64))
     flops64 = rs64.interactions * FLOPS_P2P + rs64.cell_interactions * FLOPS_CELL
@@ -817,7 +820,7 @@ def main():
         N = ht.n
         h2d = N * (40 + 88 + 64)      # geometry, velocities, rk4 inputs
         d2h = N * (56 + 48 + 24)      # dxi+tangents+normals, vels+vs, positions
-        e2e = {"value": world * n * 4 * args.steps / sec, "unit": UNIT, "h2d_bytes_per_step": h2d,
+        e2e = {"value": n_job * 4 * args.steps / sec, "unit": UNIT, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": sec / args.steps * 1e3,
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
@@ -850,7 +853,8 @@ def main():
             "config": {"workload": f"large periodic tangle: {n} points per GPU ({n_rings} rings, D=0.4 cm, "
                                    f"dl=D/800, radii U[0.02,0.05]D), 26 periodic images, Barnes-Hut "
                                    f"theta={args.theta}, mixed FP32/FP64, RK4 dt={args.dt}",
-                       "points": n, "theta": args.theta, "images": 26, "dt": args.dt,
+                       "points": n, "points_all_ranks": n_job, "theta": args.theta, "images": 26,
+                       "dt": args.dt,
                        "parallelism": f"{world} independent tangles (one per GPU)" if world > 1 else "1 GPU",
                        "l2": "working set (octree cells + node table) larger than the 126 MB L2"},
             "rk4_steps_per_s": world * 1e3 / ms_step,
