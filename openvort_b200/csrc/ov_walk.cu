@@ -329,14 +329,16 @@ __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 
 }
 
 // resident blocks per SM the register allocation must allow, measured at
-// 1M points: mixed 71.3 / 74.4 / 72.8 / 80.3 ms for 4 / 5 / 6 / 3 blocks
-// (4 blocks leave 120 registers and no spills; the FP64 form spills less
-// at 5 than its extra warps cost)
+// 1M points, ms per launch:
+//   mixed 55.5 / 53.4 / 54.6 for 4 / 5 / 6 blocks (128 registers and no
+//   spills, 96 and 100 bytes spilled, 80 and 196 bytes spilled): the extra
+//   warps hide more of the latency than the spills cost
+//   FP64 95.2 / 85.9 / 82.3 for 4 / 5 / 6 blocks
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_MIXED
-#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 4
+#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 5
 #endif
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_FP64
-#define OV_WALK_MULTI_MIN_BLOCKS_FP64 5
+#define OV_WALK_MULTI_MIN_BLOCKS_FP64 6
 #endif
 
 template <bool kMixed>
