@@ -127,3 +127,21 @@ def test_flows_restated(oracle):
         p = Params(lia_only=1, use_mf=0, hyperfriction=0, vs=Flow(name, prm))
         out = oracle.update_tangle(t, p, 0.01)
         assert np.all(np.isfinite(out.vels)), name
+
+
+@pytest.mark.skipif(not have_ref(), reason="reference library not built here")
+@pytest.mark.parametrize("use_bh,boundary", [(0, "periodic-26"), (1, "periodic-26"), (1, "periodic-18"),
+                                             (0, "open")])
+def test_oracle_vs_reference_smallest_loop(oracle, use_bh, boundary):
+    """A 5-node loop among EMPTY slots (the GPU suite's smallest case): every
+    stencil reaches round the loop and the tree has a handful of cells."""
+    from openvort_b200.tangle import ring_points
+    ref = Ref(threads=2)
+    r = ring_points(np.array([0.05, 0.05, 0.05]), (0.3, 0.2, 0.9), 0.004, 5)
+    t = G.rings_to_tangle([r], (0, 0, 0), (0.1, 0.1, 0.1), boundary, empty_slots=3)
+    p = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=1e-2, use_bh=use_bh,
+               bh_theta=0.5, vn=Flow("simple", {"external_v": (0.5, 0, 0)}))
+    a = oracle.update_tangle(t, p, 0.0)
+    b = ref.update_tangle(t, p, 0.0)
+    assert rel_err(a.vels, b.vels, t.active) < TOL_V
+    assert pos_err(oracle.rk4_step(a, p, 0.0, 1e-6).pos, ref.rk4_step(b, p, 0.0, 1e-6).pos, t.active) < 1e-14
