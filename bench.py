@@ -157,7 +157,9 @@ class Clocks:
 
 def dist_setup(args):
     from openvort_b200 import dist as D
-    r = D.setup()
+    # a rank waits at most for rank 0's accuracy checks (tens of seconds):
+    # a stuck peer ends the next collective with an error well before this
+    r = D.setup(timeout_s=180.0)
     if r.world == 1:
         import torch
         if torch.cuda.is_available():
