@@ -344,7 +344,10 @@ void ov_state_reset_stats(ov_state *s);
  * address (cudaGetSymbolAddress) with that device current; make that first
  * call before any stream capture.  All calls share the one array, which
  * keeps the last call's contents: calls whose work overlaps on the GPU (on
- * different streams, or host threads) race. */
+ * different streams, or host threads) race.  The looked-up address is kept
+ * for the life of the process: after cudaDeviceReset (or with another
+ * context made current on that device) it no longer names the array, so do
+ * not call this entry point again in that process after such a reset. */
 #define OV_NOALLOC_MAX_NODES 131072
 #define OV_NOALLOC_MAX_POINTS 131072
 #define OV_NOALLOC_MAX_POINT_IMAGES 131072
@@ -439,8 +442,12 @@ int ov_adjoint_forward(ov_adjoint *a, const double *x0, const double *vn, double
                        int nsteps, int checkpoint_every, double *x_final);
 /* cotangent of the last forward run's final positions -> cotangents of its
  * initial positions and of vn (recomputing each block of steps from its
- * checkpoint) */
+ * checkpoint, with the vn and precision that forward run used) */
 int ov_adjoint_backward(ov_adjoint *a, const double *x_final_bar, double *x0_bar, double *vn_bar);
+/* number of completed ov_adjoint_forward runs on a: a caller holding
+ * several trajectories of one handle compares it to the value after its
+ * own forward run to know whether backward still refers to that run */
+unsigned long long ov_adjoint_generation(const ov_adjoint *a);
 
 /* ----- vortex-vortex reconnection with the pair search on the GPU -----
  * The reference's pair loop (reconnect, src/vortex_dynamics.c:216-313)

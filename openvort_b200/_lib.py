@@ -35,7 +35,7 @@ FUNCTIONS = [
     "ov_batch_create", "ov_batch_destroy", "ov_batch_update", "ov_batch_run",
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
-    "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward",
+    "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward", "ov_adjoint_generation",
     "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries", "ov_eliminate_small_loops",
     "ov_save_tangle", "ov_save_frame", "ov_state_save_frame", "ov_frame_wait", "ov_frame_info",
     "ov_load_frame",
@@ -157,6 +157,7 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_adjoint_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
                                          C.c_int, C.c_int, C.c_void_p]),
         "ov_adjoint_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "ov_adjoint_generation": (C.c_ulonglong, [C.c_void_p]),
         "ov_reconnect_candidates": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p, C.c_int]),
         "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
         "ov_remesh": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p]),

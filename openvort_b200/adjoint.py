@@ -72,6 +72,11 @@ class Adjoint:
                                              t0, dt, nsteps, every, out.ctypes.data))
         return out
 
+    @property
+    def generation(self) -> int:
+        """Completed forward runs; backward refers to the last one."""
+        return int(self.lib.ov_adjoint_generation(self.h))
+
     def backward(self, x_final_bar):
         g = _arr(x_final_bar, 3 * self.n)
         xb = np.zeros((self.n, 3))
@@ -99,13 +104,21 @@ def _function():
 
         @staticmethod
         def forward(ctx, x0, vn, adj, t0, dt, nsteps, every):
-            xf = adj.forward(x0.detach().cpu().numpy(), vn.detach().cpu().numpy(), t0, dt, nsteps, every)
+            args = (x0.detach().cpu().numpy().copy(), vn.detach().cpu().numpy().copy(), t0, dt, nsteps, every)
+            xf = adj.forward(*args)
             ctx.adj = adj
+            ctx.args = args
+            ctx.generation = adj.generation
             ctx.dev = (x0.device, vn.device)
             return torch.from_numpy(xf).to(x0.device)
 
         @staticmethod
         def backward(ctx, g):
+            # another trajectory on the same handle since this one: its
+            # checkpoints are gone, so run this forward again first
+            if ctx.adj.generation != ctx.generation:
+                ctx.adj.forward(*ctx.args)
+                ctx.generation = ctx.adj.generation
             xb, vnb = ctx.adj.backward(g.detach().cpu().numpy())
             return (torch.from_numpy(xb).to(ctx.dev[0]), torch.from_numpy(vnb).to(ctx.dev[1]),
                     None, None, None, None, None)

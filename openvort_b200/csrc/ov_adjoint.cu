@@ -297,9 +297,11 @@ struct ov_adjoint {
   tangle_state hdr;
   int n = 0;
   double vn[3] = {0, 0, 0};
-  // trajectory of the last forward run
-  double t0 = 0, dt = 0;
-  int nsteps = 0, every = 1, classic = 0, have_fwd = 0;
+  // trajectory of the last forward run: its normal-fluid vector and
+  // precision are kept apart from vn, which velocity calls overwrite
+  double t0 = 0, dt = 0, fwd_vn[3] = {0, 0, 0};
+  int nsteps = 0, every = 1, classic = 0, have_fwd = 0, fwd_precision = 0;
+  unsigned long long generation = 0;
   DevBuf ckpt, blk, y[3], kv[3], kbar[4], xbar, ybar, gnl, vnbar, vn_dev, gv, tmp_dxi, tmp_tan,
       tmp_nrm, tmp_vs, tmp_v;
 };
@@ -600,7 +602,10 @@ int ov_adjoint_forward(ov_adjoint* a, const double* x0, const double* vn, double
     if (!forward_step(a, t0 + i * dt)) return ov_last_error();
   }
   if (!sync_to(a, x_final, s->pos.as<double>(), v3)) return ov_last_error();
+  for (int c = 0; c < 3; ++c) a->fwd_vn[c] = a->vn[c];
+  a->fwd_precision = s->P.precision;
   a->have_fwd = 1;
+  ++a->generation;
   return OV_OK;
 }
 
@@ -612,7 +617,11 @@ int ov_adjoint_backward(ov_adjoint* a, const double* x_final_bar, double* x0_bar
   }
   ov_state_impl* s = &a->s;
   const size_t v3 = 3 * (size_t)a->n;
-  if (!refresh(a) || !upload_pos(a, x_final_bar, a->xbar.as<double>()) ||
+  // recompute with the forward run's vn and precision, whatever velocity
+  // calls or precision changes came in between
+  if (!set_vn(a, a->fwd_vn)) return ov_last_error();
+  s->P.precision = a->fwd_precision;
+  if (!upload_pos(a, x_final_bar, a->xbar.as<double>()) ||
       !ov_cuda_ok(cudaMemsetAsync(a->vnbar.p, 0, 64, s->stream), "cudaMemsetAsync"))
     return ov_last_error();
   const int n_ckpt = (a->nsteps + a->every - 1) / a->every;
@@ -637,5 +646,7 @@ int ov_adjoint_backward(ov_adjoint* a, const double* x_final_bar, double* x0_bar
     return ov_last_error();
   return OV_OK;
 }
+
+unsigned long long ov_adjoint_generation(const ov_adjoint* a) { return a ? a->generation : 0; }
 
 }  // extern "C"

@@ -15,6 +15,7 @@
 #include <string.h>
 
 #include <atomic>
+#include <cmath>
 #include <mutex>
 #include <string>
 
@@ -456,17 +457,14 @@ static bool upload_tangle(ov_state_impl* s, const tangle_state* t, bool need_flo
     ov_set_error(OV_ERR_INVALID, "null tangle");
     return false;
   }
-  if (!ensure_init()) return false;
-  if (!capture_params(t, s->P, need_flows)) return false;
-  if (!ov_state_reserve(s, t->N)) return false;
   size_t n = (size_t)t->N;
   // targets (non-EMPTY, non-PINNED) and segments (forward link) for the
   // interaction counts of the direct sum
   // and a check that every link and wall index the kernels follow is in
   // range, so a malformed tangle is an error instead of a stray device read
   int nt = 0, ns = 0, na = 0;
-  if (t->N > 0 && (!t->status || !t->connections)) {
-    ov_set_error(OV_ERR_INVALID, "tangle without status or connection arrays");
+  if (t->N > 0 && (!t->status || !t->connections || !t->vnodes)) {
+    ov_set_error(OV_ERR_INVALID, "tangle without status, connection or position arrays");
     return false;
   }
   for (int k = 0; k < t->N; ++k) {
@@ -481,10 +479,22 @@ static bool upload_tangle(ov_state_impl* s, const tangle_state* t, bool need_flo
                    f, r, (int)t->status[k].pin_wall);
       return false;
     }
+    // a NaN or infinite position of a live node is refused here, before any
+    // launch, so no output array is written (EMPTY slots may hold anything)
+    const vec3d& x = t->vnodes[k];
+    if (!(std::isfinite(x.p[0]) && std::isfinite(x.p[1]) && std::isfinite(x.p[2]))) {
+      ov_set_error(OV_ERR_NONFINITE, "node %d: non-finite position (%g, %g, %g)", k, x.p[0], x.p[1],
+                   x.p[2]);
+      return false;
+    }
     ++na;
     if (st != PINNED) ++nt;
     if (f >= 0) ++ns;
   }
+  // the host arrays are valid: now the device
+  if (!ensure_init()) return false;
+  if (!capture_params(t, s->P, need_flows)) return false;
+  if (!ov_state_reserve(s, t->N)) return false;
   s->n_targets = nt;
   s->n_segments = ns;
   s->n_active = na;

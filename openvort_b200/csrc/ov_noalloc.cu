@@ -28,7 +28,9 @@ std::mutex g_mutex;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 
 // Device address of g_scratch on the current device, looked up on the first
-// call per device (with that device current) and kept.
+// call per device (with that device current) and kept for the life of the
+// process; a cudaDeviceReset of that device makes the kept address stale,
+// which the entry point's documentation rules out.
 bool scratch_address(unsigned char** out) {
   int dev = -1;
   if (!ov_cuda_ok(cudaGetDevice(&dev), "cudaGetDevice")) return false;

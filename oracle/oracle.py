@@ -23,7 +23,9 @@ from openvort_b200.tangle import FLOW_KINDS, FLOW_PARAMS, IMAGE_TABLES, HostTang
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "liboracle.so"
 REF_SO = HERE / "_ref" / "libov_ref.so"
-REF_SRC = Path("/root/reference")
+# the reference checkout the recipe compiles from: $OPENVORT_REF, by default
+# the read-only checkout of the machine that builds the checkers
+REF_SRC = Path(os.environ.get("OPENVORT_REF", "/root/reference"))
 
 
 def build(ref: bool = True):
@@ -32,7 +34,7 @@ def build(ref: bool = True):
     targets = ["liboracle.so"]
     if ref and (REF_SRC / "src" / "tangle.c").exists():
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REF_SRC}", *targets], check=True)
 
 
 # ---------------------------------------------------------------- restatement

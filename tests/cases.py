@@ -51,3 +51,9 @@ def pos_err(a, b, mask=None) -> float:
         a, b = a[mask], b[mask]
     scale = max(1e-30, float(np.max(np.abs(b))))
     return float(np.max(np.abs(a - b))) / scale
+
+
+def fixture_flows(meta: dict):
+    """(index, Flow) of each flow recorded in a flows fixture."""
+    return [(i, Flow(f["name"], {n: (tuple(v) if isinstance(v, list) else v) for n, v in f["params"].items()}))
+            for i, f in enumerate(meta["flows"])]

@@ -70,10 +70,70 @@ def cases():
     yield "periodic_z_flows", t3, p3, {"rk4_steps": 1, "dt": 1e-6, "time": 0.003}
 
 
+# Every flow of the reference's table (src/external_velocity.c:85-174) with
+# parameters that make it non-trivial on the flows tangle (centres in
+# [0, 0.1]^3, evaluated at t = 3 ms).  "spherical and simple" is absent: the
+# reference's function returns before writing its output (get_v_simple
+# returns 1, read as an error at :235-237), so update_velocity adds an
+# uninitialised stack value; tests/test_oracle.py pins that behaviour and the
+# GPU's sum of the two flows is checked against the two recorded separately.
+FLOWS16 = [
+    ("no flow", {}),
+    ("spherical", {"strength": 2e-3, "cutoff": 0.02}),
+    ("simple", {"external_v": (0.3, -0.1, 0.2)}),
+    ("cylindrical", {"strength": 2e-3, "cutoff": 0.02}),
+    ("oscillating", {"strength": 0.3, "frequency": 50.0, "wave": (10.0, 3.0, 5.0),
+                     "polarization": (0.2, 1.0, -0.4)}),
+    ("oscillating slit", {"strength": 0.4, "frequency": 40.0, "cutoff": 0.03}),
+    ("coscos", {"k": 50.0, "v0": 0.1, "l": 0.05}),
+    ("coscos-divfree", {"k": 50.0, "v0": 0.1, "l": 0.05}),
+    ("cos-divfree", {"k": 40.0, "v0": 0.2, "l": 0.07}),
+    ("simple-shear", {"rate": 3.0, "v0": 0.1}),
+    ("rotosc", {"freq": 20.0, "amp": 0.5}),
+    ("DG", {"rot": 2.0, "vz": 0.1}),
+    ("rotosc-boundary", {"freq": 30.0, "amp": 0.7}),
+    ("constant acceleration", {"accel": 30.0}),
+    ("parabolic", {"H": 0.1, "amp": 20.0}),
+]
+FLOWS_TIME = 0.003
+
+
+def flows16(ref):
+    """One tangle, each flow once as vn_conf (mutual friction) and once as
+    vs_conf; the fixture's base arrays are the no-flow run."""
+    t = G.random_ring_tangle(7, 5, 0.1, boundary="open")
+    t.box_lo, t.box_hi = (-0.05,) * 3, (0.15,) * 3
+    t._bind()
+    base = Params(core_a=1e-8, alpha=0.1, alpha_p=0.02, dl_max=1e-3, hyperfriction=0,
+                  vn=Flow("no flow"), vs=Flow("no flow"))
+    u = ref.update_tangle(t, base, FLOWS_TIME)
+    arrays = dict(pos=t.pos, fwd=t.links[:, 0], rev=t.links[:, 1], status=t.stat[:, 0],
+                  pin_wall=t.stat[:, 1], box_lo=np.array(t.box_lo), box_hi=np.array(t.box_hi),
+                  dxi=u.dxi, tangents=u.tangents, normals=u.normals, vels=u.vels, vs=u.vs)
+    for i, (fname, prm) in enumerate(FLOWS16):
+        for which in ("vn", "vs"):
+            p = dataclasses.replace(base, **{which: Flow(fname, prm)})
+            r = ref.update_tangle(t, p, FLOWS_TIME)
+            arrays[f"vels_{which}_{i}"] = r.vels
+            if which == "vs":       # vn_conf enters only vels
+                arrays[f"vs_{which}_{i}"] = r.vs
+    flows = [{"name": n, "params": {k: (list(v) if isinstance(v, tuple) else v) for k, v in prm.items()}}
+             for n, prm in FLOWS16]
+    meta = {"boundary": t.boundary, "params": json.loads(params_json(base)), "time": FLOWS_TIME,
+            "rk4_steps": 0, "dt": 0, "flows": flows}
+    np.savez_compressed(OUT / "flows16.npz", meta=np.array(json.dumps(meta)), **arrays)
+    print("flows16", t.n, "nodes")
+
+
 def main():
     build()
     ref = Ref(threads=8)
+    only = sys.argv[1:]
+    if not only or "flows16" in only:
+        flows16(ref)
     for name, t, p, opt in cases():
+        if only and name not in only:
+            continue
         time = opt.get("time", 0.0)
         u = ref.update_tangle(t, p, time)
         arrays = dict(pos=t.pos, fwd=t.links[:, 0], rev=t.links[:, 1], status=t.stat[:, 0],

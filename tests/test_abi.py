@@ -14,7 +14,7 @@ import pytest
 from openvort_b200 import _lib, geometry as G
 from openvort_b200.tangle import (BOUNDARY_SYMBOLS, IMAGE_TABLES, BoundaryImages, NodeStatus,
                                   Neighbour, Params, TangleState, VConf, Vec3d)
-from oracle.oracle import REF_SO, have_ref
+from oracle.oracle import REF_SO, REF_SRC, have_ref
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "openvort_b200.h"
@@ -95,15 +95,15 @@ def test_struct_layouts(tmp_path):
     assert vals == py
 
 
-@pytest.mark.skipif(not Path("/root/reference/include/tangle.h").exists(),
-                    reason="reference headers absent")
+@pytest.mark.skipif(not (REF_SRC / "include" / "tangle.h").exists(),
+                    reason="reference headers absent ($OPENVORT_REF)")
 def test_header_interchangeable_with_reference(tmp_path):
     """The reference's headers and this one compile together in either order."""
     for order in (("tangle.h", "openvort_b200.h"), ("openvort_b200.h", "tangle.h")):
         src = tmp_path / "both.c"
         src.write_text("".join(f'#include "{h}"\n' for h in order) + "int main(void){return 0;}\n")
         subprocess.run(["gcc", "-fsyntax-only", "-I", str(ROOT / "include"),
-                        "-I", "/root/reference/include", str(src)], check=True)
+                        "-I", str(REF_SRC / "include"), str(src)], check=True)
 
 
 def _table(lib, sym):
@@ -157,3 +157,36 @@ def test_no_gpu_fails_loudly(lib, monkeypatch):
     assert lib.ov_init(0) == _lib.OV_ERR_NO_DEVICE
     peak = C.c_double(0)
     assert lib.ov_measure_fma_peak(0, C.byref(peak)) != 0
+
+
+@pytest.mark.parametrize("value", [np.nan, np.inf])
+def test_nonfinite_position_is_refused_before_any_work(lib, monkeypatch, value):
+    """A live node at a NaN or infinite position makes every reference-named
+    call return OV_ERR_NONFINITE from the host-side check, before the device
+    is touched, with every output array left as it was."""
+    monkeypatch.setenv("OV_QUIET", "1")
+    import openvort_b200 as ov
+    t = G.single_ring(32, 1e-2)
+    ov.configure(Params(use_mf=0, hyperfriction=0))
+    t.pos[5, 1] = value
+    for arr in (t.vels, t.tangents, t.normals):
+        arr[:] = 7.0
+    pos0 = t.pos.copy()
+    for call in (lambda: ov.update_velocities(t, 0.0), lambda: ov.rk4_step(t, 0.0, 1e-6),
+                 lambda: ov.update_tangents_normals(t), lambda: ov.update_tangle(t, 0.0)):
+        with pytest.raises(ov.OVError) as e:
+            call()
+        assert e.value.code == _lib.OV_ERR_NONFINITE
+        lib.ov_clear_error()
+    assert np.all(t.vels == 7.0) and np.all(t.tangents == 7.0) and np.all(t.normals == 7.0)
+    assert np.array_equal(t.pos, pos0, equal_nan=True)
+    # an EMPTY slot may hold anything
+    t2 = G.single_ring(32, 1e-2)
+    t2.stat[31, 0] = -1   # EMPTY
+    t2.links[30, 0] = 0
+    t2.links[0, 1] = 30
+    t2.pos[31] = value
+    try:
+        ov.update_tangents_normals(t2)
+    except ov.OVError as e:
+        assert e.code != _lib.OV_ERR_NONFINITE

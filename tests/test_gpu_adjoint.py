@@ -149,6 +149,44 @@ def test_checkpoint_interval_changes_nothing(adj):
         assert np.max(np.abs(v - v1)) <= 1e-13 * np.max(np.abs(v1))
 
 
+def test_interleaved_trajectories_keep_their_own_gradients(adj):
+    """Two trajectories of one handle, and a velocity call with another vn,
+    before either backward: each gradient equals that of its run alone."""
+    import torch
+    from openvort_b200.adjoint import centroid_length_loss, trajectory
+    t, a = adj
+    g1, v1 = _grads(a, t, every=8)
+    x0 = torch.tensor(t.pos, dtype=torch.float64, requires_grad=True)
+    vn = torch.tensor(VN, dtype=torch.float64, requires_grad=True)
+    xf = trajectory(a, x0, vn, 0.0, DT, STEPS, 8)
+    x0b = torch.tensor(t.pos * 1.01, dtype=torch.float64, requires_grad=True)
+    vnb = torch.tensor(3 * VN, dtype=torch.float64, requires_grad=True)
+    xfb = trajectory(a, x0b, vnb, 0.0, DT, STEPS, 4)
+    a.velocity(t.pos, -VN)
+    centroid_length_loss(xf, t.links[:, 0], t.active, TARGET).backward()
+    assert np.max(np.abs(x0.grad.numpy() - g1)) <= 1e-13 * np.max(np.abs(g1))
+    assert np.max(np.abs(vn.grad.numpy() - v1)) <= 1e-13 * np.max(np.abs(v1))
+    centroid_length_loss(xfb, t.links[:, 0], t.active, TARGET).backward()
+    x0c = torch.tensor(t.pos * 1.01, dtype=torch.float64, requires_grad=True)
+    vnc = torch.tensor(3 * VN, dtype=torch.float64, requires_grad=True)
+    centroid_length_loss(trajectory(a, x0c, vnc, 0.0, DT, STEPS, 4), t.links[:, 0], t.active,
+                         TARGET).backward()
+    assert np.max(np.abs(x0b.grad.numpy() - x0c.grad.numpy())) <= 1e-13 * np.max(np.abs(x0c.grad.numpy()))
+    assert np.max(np.abs(vnb.grad.numpy() - vnc.grad.numpy())) <= 1e-13 * np.max(np.abs(vnc.grad.numpy()))
+
+
+def test_backward_uses_the_forward_runs_vn(adj):
+    """Through the C ABI: a velocity call with another vn between forward
+    and backward changes no cotangent."""
+    t, a = adj
+    g = np.random.default_rng(3).normal(size=(N, 3))
+    a.forward(t.pos, VN, 0.0, DT, STEPS, 8)
+    xb1, vb1 = a.backward(g)
+    a.velocity(t.pos, 5 * VN)
+    xb2, vb2 = a.backward(g)
+    assert np.array_equal(xb1, xb2) and np.array_equal(vb1, vb2)
+
+
 def test_adjoint_rejects_unsupported_tangles(ov, monkeypatch):
     monkeypatch.setenv("OV_QUIET", "1")
     lib = ov.load()

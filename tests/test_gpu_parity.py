@@ -14,7 +14,7 @@ import dataclasses
 import numpy as np
 import pytest
 
-from cases import NAMES, load, pos_err, rel_err
+from cases import NAMES, fixture_flows, load, pos_err, rel_err
 from openvort_b200 import geometry as G
 from openvort_b200.tangle import Flow, Params, Vec3d
 from oracle.oracle import Oracle
@@ -77,6 +77,40 @@ def test_rk4_fp64_vs_golden(ov, name):
         tt += meta["dt"]
         ov.update_tangle(cur, tt)
         assert pos_err(cur.pos, z[f"rk4_pos_{s + 1}"], t.active) < 1e-14
+
+
+@pytest.mark.parametrize("which", ["vn", "vs"])
+def test_all_external_flows_fp64_vs_reference(ov, which):
+    """Each flow of the reference's table (src/external_velocity.c:85-174)
+    as vn_conf (through mutual friction) and as vs_conf, FP64, against the
+    reference's own update_tangle on the same tangle and time."""
+    t, base, meta, z = load("flows16")
+    act = t.active
+    flows = fixture_flows(meta)
+    assert len(flows) == 15
+    for i, f in flows:
+        out = gpu_update(ov, t, dataclasses.replace(base, **{which: f}), meta["time"])
+        assert rel_err(out.vels, z[f"vels_{which}_{i}"], act) < TOL_V64, f.name
+        want_vs = z[f"vs_vs_{i}"] if which == "vs" else z["vs"]
+        assert rel_err(out.vs, want_vs, act) < TOL_V64, f.name
+
+
+@pytest.mark.parametrize("which", ["vn", "vs"])
+def test_spherical_and_simple_is_the_sum_of_its_parts(ov, which):
+    """The reference's "spherical and simple" returns before writing its
+    output (src/external_velocity.c:226-237), so its own result is an
+    uninitialised value.  The library gives spherical + simple: since vs and
+    vels are affine in the external flow, that equals the reference's
+    spherical run plus its simple run minus its no-flow run."""
+    t, base, meta, z = load("flows16")
+    act = t.active
+    idx = {f.name: (i, f) for i, f in fixture_flows(meta)}
+    (i_sph, sph), (i_sim, sim), (i_0, _) = idx["spherical"], idx["simple"], idx["no flow"]
+    assert sph.params["cutoff"] > 0
+    both = Flow("spherical and simple", {**sph.params, **sim.params})
+    out = gpu_update(ov, t, dataclasses.replace(base, **{which: both}), meta["time"])
+    want = z[f"vels_{which}_{i_sph}"] + z[f"vels_{which}_{i_sim}"] - z[f"vels_{which}_{i_0}"]
+    assert rel_err(out.vels, want, act) < TOL_V64
 
 
 def test_device_state_run_vs_oracle(ov, oracle):

@@ -6,7 +6,7 @@ import pytest
 
 from cases import NAMES, load, pos_err, rel_err
 from openvort_b200 import geometry as G
-from openvort_b200.tangle import Flow, Params
+from openvort_b200.tangle import FLOW_PARAMS, Flow, Params
 from oracle.oracle import Oracle, Ref, have_ref
 
 # FP64 parity bound on velocities (max over nodes of |dv| / |v_ref|)
@@ -104,6 +104,44 @@ def test_oracle_point_queries_vs_reference(oracle):
     skip = rng.integers(-1, t.n, size=64).astype(np.int32)
     assert rel_err(oracle.segments_at(t, p, pts, skip), ref.segments_at(t, p, pts, skip)) < TOL_V
     assert rel_err(oracle.bh_at(t, p, pts, skip), ref.bh_at(t, p, pts, skip)) < TOL_V
+
+
+def test_oracle_flows_match_reference_fixture(oracle):
+    """The restated flows against the reference's update_tangle with each
+    flow of its table as vn_conf and as vs_conf (flows16 fixture)."""
+    import dataclasses
+    from cases import fixture_flows
+    t, base, meta, z = load("flows16")
+    act = t.active
+    for i, f in fixture_flows(meta):
+        for which in ("vn", "vs"):
+            out = oracle.update_tangle(t, dataclasses.replace(base, **{which: f}), meta["time"])
+            assert rel_err(out.vels, z[f"vels_{which}_{i}"], act) < TOL_V, (f.name, which)
+
+
+@pytest.mark.skipif(not have_ref(), reason="reference library not built here")
+def test_reference_spherical_and_simple_leaves_its_output_unwritten():
+    """Pins the reference's behaviour behind the library's one deviation:
+    get_v_spherical_and_simple (src/external_velocity.c:226-237) returns the
+    1 of get_v_simple as an error before adding the two flows, so the
+    caller's vector keeps whatever it held.  Its two parts each write."""
+    import ctypes as C
+    from openvort_b200.tangle import Vec3d
+    ref = Ref(threads=1)
+    prm = {"external_v": (0.3, -0.1, 0.2), "strength": 2e-3, "cutoff": 0.02}
+    where = Vec3d((0.03, 0.02, 0.01))
+    for fname, fn, want_rc, writes in (("spherical and simple", "get_v_spherical_and_simple", 1, False),
+                                       ("spherical", "get_v_spherical", 0, True),
+                                       ("simple", "get_v_simple", 1, True)):
+        conf, keep = Flow(fname, {k: v for k, v in prm.items()
+                                  if k in dict(FLOW_PARAMS[fname])}).vconf()
+        res = Vec3d((-7.0, -7.0, -7.0))
+        f = getattr(ref.lib, fn)
+        f.restype = C.c_int
+        f.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]
+        rc = f(C.addressof(where), 0.0, C.addressof(res), C.addressof(conf))
+        assert rc == want_rc, fname
+        assert (list(res.p) != [-7.0] * 3) == writes, fname
 
 
 def test_flows_restated(oracle):
