@@ -77,9 +77,14 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the direct-sum and batch lines")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--cfg1-steps", type=int, default=1000)
+    ap.add_argument("--cfg2-steps", type=int, default=500)
+    ap.add_argument("--cfg2-direct-steps", type=int, default=20)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--shard", action="store_true",
-                    help="one tangle over all ranks (targets split, sums all-gathered) instead of one per rank")
+                    help="at one GPU too: the sharded one-tangle run (the default when --gpus > 1)")
+    ap.add_argument("--independent", action="store_true",
+                    help="with --gpus > 1: one independent tangle per rank (weak scaling) as the headline")
     return ap.parse_args()
 
 
@@ -215,6 +220,17 @@ def cpu_reference_sample(tangle, p, target_s=10.0, time0=0.0):
                        f"of all nodes: {t_eval:.1f} s")}
 
 
+def bench_config(args, n, n_job, n_rings, world) -> dict:
+    """The workload description both arms print."""
+    return {"workload": f"large periodic tangle: {n} points per GPU ({n_rings} rings, D=0.4 cm, "
+                        f"dl=D/800, radii U[0.02,0.05]D), 26 periodic images, Barnes-Hut "
+                        f"theta={args.theta}, mixed FP32/FP64, RK4 dt={args.dt}",
+            "points": n, "points_all_ranks": n_job, "theta": args.theta, "images": 26,
+            "dt": args.dt,
+            "parallelism": f"{world} independent tangles (one per GPU)" if world > 1 else "1 GPU",
+            "l2": "working set (octree cells + node table) larger than the 126 MB L2"}
+
+
 def run_reference_arm(args, world, rank):
     p = params(args.theta)
     tangle, n_rings = make_tangle(args.points, args.seed)
@@ -222,6 +238,7 @@ def run_reference_arm(args, world, rank):
     # warm-up samples are small; each timed step is one sampled evaluation
     for _ in range(args.warmup):
         cpu_reference_sample(tangle, p, target_s=0.5)
+    t0 = time.perf_counter()
     for _ in range(args.steps):
         r = cpu_reference_sample(tangle, p, target_s=8.0)
         if r is None:
@@ -229,19 +246,80 @@ def run_reference_arm(args, world, rank):
                               "unavailable": "oracle/_ref/libov_ref.so (reference compiled from its sources) is not built"}))
             return
         vals.append(r)
+    timed_s = time.perf_counter() - t0
     v = statistics.median([r["value"] for r in vals])
     n = int(tangle.active.sum())
     ms_step = 4 * n / v * 1e3
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"large periodic tangle, {n} points ({n_rings} rings, D=0.4 cm, dl=D/800), "
-                                   f"26 images, Barnes-Hut theta={args.theta}", "points": n,
-                       "theta": args.theta},
+            "config": bench_config(args, n, n, n_rings, world),
+            "extrapolated": True,
+            "timed_s": timed_s,
+            "step_meaning": (f"each of the {args.steps} timed steps is one sampled evaluation (see "
+                             "cpu_baseline.sample) extrapolated to all nodes; ms_per_step is the RK4 step "
+                             "(4 evaluations) those samples imply, not wall time"),
             "rk4_steps_per_s": 1e3 / ms_step,
             "cpu_baseline": {**vals[-1], "value": v},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def dist_stats(e: np.ndarray) -> dict:
+    return {"max": float(np.max(e)), "p99": float(np.percentile(e, 99)), "median": float(np.median(e))}
+
+
+def bh_reference_check(tangle, p, idx, bh64, direct, vs64, n_direct=64):
+    """The reference's own Barnes-Hut error on the sample nodes: its
+    update_velocity (oracle/_ref) with its octree at all sample nodes, and
+    with its direct sum at the first n_direct of them.  Reported beside the
+    GPU's FP64 Barnes-Hut and direct sums at the same nodes, all relative to
+    the direct-sum superfluid velocity."""
+    from oracle.oracle import Ref, have_ref
+    if not have_ref():
+        return None
+    ref = Ref(threads=os.cpu_count() or 1)
+    ref.configure(p)
+    t = tangle.copy()
+    t.set_images_from_library(ref.lib)
+    ref.lib.update_tangents_normals.restype = None
+    ref.lib.update_tangents_normals(C.cast(t.ptr(), C.c_void_p))
+    f = ref.lib.refh_sample_vs
+    f.restype = None
+    f.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_double)]
+    idx = np.ascontiguousarray(idx, dtype=np.int32)
+    m = len(idx)
+    tb = C.c_double()
+    t0 = time.perf_counter()
+    ref_bh = np.zeros((m, 3))
+    f(C.cast(t.ptr(), C.c_void_p), 0.0, idx.ctypes.data, m, 1, ref_bh.ctypes.data, C.byref(tb))
+    t1 = time.perf_counter()
+    nd = min(n_direct, m)
+    ref_direct = np.zeros((nd, 3))
+    f(C.cast(t.ptr(), C.c_void_p), 0.0, idx.ctypes.data, nd, 0, ref_direct.ctypes.data, C.byref(tb))
+    t2 = time.perf_counter()
+    # GPU superfluid velocities at the sample nodes: FP64 with the tree, and
+    # with the direct sum in place of the tree's Biot-Savart sum
+    gpu_bh = vs64[idx]
+    gpu_direct = vs64[idx] - bh64 + direct
+    norm = np.linalg.norm(gpu_direct, axis=1)
+
+    def rel(a, b, k=None):
+        k = len(a) if k is None else k
+        return np.linalg.norm(a[:k] - b[:k], axis=1) / norm[:k]
+    return {
+        "nodes": m, "direct_nodes": nd,
+        "reference_bh_vs_reference_direct": dist_stats(rel(ref_bh, ref_direct, nd)),
+        "gpu_bh_fp64_vs_gpu_direct_same_nodes": dist_stats(rel(gpu_bh, gpu_direct, nd)),
+        "reference_bh_vs_gpu_direct": dist_stats(rel(ref_bh, gpu_direct)),
+        "gpu_bh_fp64_vs_gpu_direct": dist_stats(rel(gpu_bh, gpu_direct)),
+        "gpu_bh_fp64_vs_reference_bh": dist_stats(rel(gpu_bh, ref_bh)),
+        "gpu_direct_vs_reference_direct": dist_stats(rel(gpu_direct, ref_direct, nd)),
+        "reference_seconds": {"bh_with_build": t1 - t0, "build": tb.value, "direct": t2 - t1},
+        "what": ("superfluid velocity vs (local term + flow + Biot-Savart + 26 images) at seeded sample "
+                 "nodes; errors are |a - b| / |vs with the direct sum|; the reference's update_velocity "
+                 "from oracle/_ref with its own octree (all nodes) and its direct sum (first direct_nodes)"),
+    }
 
 
 # ---------------------------------------------------------------- GPU side
@@ -316,6 +394,97 @@ def bench_direct(args, ov, peak32: float, peak64: float):
     out["max_rel_err_mixed_vs_fp64"] = float(np.max(num / den))
     out["mixed_over_fp64_speedup"] = out["fp64"]["kernel_ms"] / out["mixed"]["kernel_ms"]
     return out
+
+
+def bench_cfg2(args, ov):
+    """The 22.4k-point periodic tangle (512 rings in a periodic cube D = 0.1
+    cm, radii U[0.02, 0.05] D, dl = D/200, 26 images, counterflow 0.5 cm/s,
+    alpha 0.098, alpha' 0.016) stepped with RK4 at dt = 1e-6 s, device
+    resident: the direct sum and Barnes-Hut at theta = 0.4, each in FP64 and
+    mixed.  The Barnes-Hut forms run the config's 500 steps; the direct sums
+    a stated subset (their per-step time is steady).  Errors: Barnes-Hut vs
+    direct (the approximation the reference makes) and mixed vs FP64, over
+    all nodes after update_tangle."""
+    from openvort_b200 import geometry as G
+    from openvort_b200.tangle import Flow, Params
+    D2 = 0.1
+    dl2 = D2 / 200
+    t = G.random_ring_tangle(args.seed + 2, 512, D2, dl=dl2, boundary="periodic-26")
+    n = int(t.active.sum())
+    base = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=2 * dl2, hyperfriction=1,
+                  use_bh=0, bh_theta=0.4, bh_grain=1e-8, vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}),
+                  vs=Flow("no flow"))
+    import dataclasses
+    steps = {("direct", "fp64"): args.cfg2_direct_steps, ("direct", "mixed"): args.cfg2_direct_steps,
+             ("bh", "fp64"): args.cfg2_steps, ("bh", "mixed"): args.cfg2_steps}
+    out = {"workload": f"512 rings, {n} points, periodic cube D=0.1 cm, dl=D/200, 26 images, counterflow "
+                       f"0.5 cm/s, RK4 dt=1e-6 s; direct sum and Barnes-Hut theta=0.4, FP64 and mixed",
+           "points": n}
+    vels = {}
+    for method, use_bh in (("direct", 0), ("bh", 1)):
+        p = dataclasses.replace(base, use_bh=use_bh)
+        for form, prec in (("fp64", ov.OV_PREC_FP64), ("mixed", ov.OV_PREC_MIXED)):
+            ov.configure(p, prec)
+            s = ov.DeviceState(t.copy())
+            s.update_tangle(0.0)
+            s.download()
+            vels[(method, form)] = s.t.vels.copy()
+            s.close()
+            k = steps[(method, form)]
+            st = ov.DeviceState(t.copy())
+            st.run(0.0, 1e-6, 1)
+            st.reset_stats()
+            st.run(1e-6, 1e-6, k)
+            rs = st.stats()
+            st.close()
+            ms = rs.last_run_ms / k
+            out[f"{method}_{form}"] = {"steps": k, "ms_per_step": ms, "rk4_steps_per_s": 1e3 / ms,
+                                       "point_evals_per_s": n * 4 / (ms / 1e3)}
+    act = t.active
+
+    def rel(a, b):
+        return float(np.max(np.linalg.norm(a[act] - b[act], axis=1) / np.linalg.norm(b[act], axis=1)))
+    out["max_rel_err_bh_vs_direct_fp64"] = rel(vels[("bh", "fp64")], vels[("direct", "fp64")])
+    out["max_rel_err_mixed_vs_fp64_direct"] = rel(vels[("direct", "mixed")], vels[("direct", "fp64")])
+    out["max_rel_err_mixed_vs_fp64_bh"] = rel(vels[("bh", "mixed")], vels[("bh", "fp64")])
+    out["bh_over_direct_speedup_fp64"] = out["direct_fp64"]["ms_per_step"] / out["bh_fp64"]["ms_per_step"]
+    out["mixed_over_fp64_speedup_bh"] = out["bh_fp64"]["ms_per_step"] / out["bh_mixed"]["ms_per_step"]
+    ov.configure(params(args.theta), ov.OV_PREC_MIXED)
+    return out
+
+
+def bench_cfg1(args, ov):
+    """The 256-point ring (R = 1e-2 cm, open boundaries, T = 0: no mutual
+    friction, a = 1.3e-8 cm, direct FP64 sum) stepped 1000 times with RK4 at
+    dt = 5e-6 s, device resident, and its speed against the thin-core
+    formula kappa/(4 pi R)(ln(8R/a) - 1/2).  dl_max = 2 dl keeps the
+    hyperfriction threshold above the ring's curvature; with remeshing at
+    [0.5, 2] dl and reconnection nothing would change on a single ring."""
+    from openvort_b200 import geometry as G
+    from openvort_b200.tangle import Params
+    R, a, kappa, n, dt, steps = 1e-2, 1.3e-8, 9.97e-4, 256, 5e-6, args.cfg1_steps
+    dl = 2 * np.pi * R / n
+    p = Params(kappa=kappa, core_a=a, use_mf=0, alpha=0.0, alpha_p=0.0, hyperfriction=1, dl_max=2 * dl,
+               use_bh=0)
+    t = G.single_ring(n, R)
+    ov.configure(p, ov.OV_PREC_FP64)
+    st = ov.DeviceState(t.copy())
+    st.reset_stats()
+    st.run(0.0, dt, steps)
+    rs = st.stats()
+    st.download()
+    z1 = float(st.t.pos[:, 2].mean())
+    radius = float(np.mean(np.linalg.norm(st.t.pos[:, :2], axis=1)))
+    st.close()
+    v = z1 / (steps * dt)
+    v_thin = kappa / (4 * np.pi * R) * (np.log(8 * R / a) - 0.5)
+    ms = rs.last_run_ms / steps
+    ov.configure(params(args.theta), ov.OV_PREC_MIXED)
+    return {"workload": f"one ring, R=1e-2 cm, {n} points, open, T=0, a=1.3e-8 cm, direct FP64, RK4 "
+                        f"dt=5e-6 s, {steps} steps", "steps": steps, "ms_per_step": ms,
+            "rk4_steps_per_s": 1e3 / ms, "point_evals_per_s": n * 4 / (ms / 1e3),
+            "ring_speed_cm_s": v, "thin_core_speed_cm_s": v_thin, "speed_over_thin_core": v / v_thin,
+            "radius_drift": radius / R - 1}
 
 
 def bench_batch(args, ov, peak32: float):
@@ -621,6 +790,29 @@ def bench_frames(args, ov, tangle, p):
     return out
 
 
+def independent_tangles(args, ov, p, dist, rank, world):
+    """Weak-scaling figures beside the sharded headline: every rank steps its
+    own seeded tangle of the same size, no collective on the data path."""
+    from openvort_b200.dist import rank_seed
+    t, _ = make_tangle(args.points, rank_seed(args.seed, rank))
+    n = int(t.active.sum())
+    ov.configure(p, ov.OV_PREC_MIXED)
+    st = ov.DeviceState(t.copy())
+    st.run(0.0, args.dt, 1)
+    barrier(dist)
+    st.reset_stats()
+    barrier(dist)
+    st.run(args.dt, args.dt, args.steps)
+    barrier(dist)
+    ms = max_over_ranks(dist, st.stats().last_run_ms) / args.steps
+    st.close()
+    from openvort_b200.dist import sum_over_ranks
+    n_job = int(round(sum_over_ranks(dist, float(n))))
+    return {"scaling": "weak", "points_all_ranks": n_job, "ms_per_step": ms,
+            "value": n_job * 4 / (ms / 1e3), "unit": UNIT,
+            "parallelism": f"{world} independent tangles (one per GPU), no collective on the data path"}
+
+
 def run_sharded(args, world, rank, local, dist):
     """One tangle over all ranks (openvort_b200.shard): every rank holds the
     same tangle and builds the same tree, walks its share of the targets, and
@@ -660,10 +852,37 @@ def run_sharded(args, world, rank, local, dist):
     rs = st.stats()
     walk_ms = max_over_ranks(dist, rs.bs_kernel_ms / max(1.0, rs.bs_launches))
     cells = D.sum_over_ranks(dist, rs.cell_interactions)
+    p2p = D.sum_over_ranks(dist, rs.interactions)
     launches = int(rs.launches)
+    # end to end through the public API: each step uploads the tangle from
+    # pinned host memory, runs the sharded step and reads the positions back
+    e2e = None
+    if not args.no_e2e:
+        alloc, keep = pinned_alloc()
+        ht = tangle.copy(alloc=alloc)
+        st.t = ht
+        barrier(dist)
+        t0 = time.perf_counter()
+        tt = (args.warmup + args.steps) * args.dt
+        for _ in range(args.steps):
+            st.upload()
+            run.step(tt, args.dt)
+            st.download(ov.OV_FIELD_POS)
+            tt += args.dt
+        barrier(dist)
+        sec = max_over_ranks(dist, time.perf_counter() - t0)
+        e2e = {"value": n * 4 * args.steps / sec, "unit": UNIT, "h2d_bytes_per_step": ht.n * (24 + 8 + 8),
+               "d2h_bytes_per_step": ht.n * 24, "ms_per_step": sec / args.steps * 1e3,
+               "path": "DeviceState.upload from pinned host memory + sharded RK4 step + positions read back"}
     st.close()
+    indep = None if args.no_extra or world == 1 else independent_tangles(args, ov, p, dist, rank, world)
     if rank == 0:
         ms_step = ms_run / args.steps
+        peak32 = C.c_double(0)
+        lib.ov_measure_fma_peak(0, C.byref(peak32))
+        launches_walk = max(1.0, rs.bs_launches)
+        flops = (p2p * FLOPS_P2P + cells * FLOPS_CELL) / launches_walk
+        achieved = flops / (walk_ms / 1e3) / 1e12 / world
         print(json.dumps({
             "metric": METRIC, "value": n * 4 * args.steps / (ms_run / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
@@ -671,15 +890,20 @@ def run_sharded(args, world, rank, local, dist):
             "config": {"workload": f"large periodic tangle: {n} points ({n_rings} rings, D=0.4 cm, dl=D/800, "
                                    f"radii U[0.02,0.05]D), 26 periodic images, Barnes-Hut theta={args.theta}, "
                                    f"mixed FP32/FP64, RK4 dt={args.dt}",
-                       "points": n, "theta": args.theta, "images": 26, "dt": args.dt,
+                       "points": n, "points_all_ranks": n, "theta": args.theta, "images": 26, "dt": args.dt,
                        "parallelism": f"one tangle over {world} ranks: each walks 1/{world} of the targets "
                                       f"in tree key order, Biot-Savart sums all-gathered per evaluation",
                        "l2": "working set (octree cells + node table) larger than the 126 MB L2"},
             "rk4_steps_per_s": 1e3 / ms_step,
             "walk_ms_per_launch_max_over_ranks": walk_ms,
-            "cell_interactions_per_point": cells / max(1.0, rs.bs_launches) / n,
+            "cell_interactions_per_point": cells / launches_walk / n,
             "exchange_bytes_per_evaluation": 48 * n,
-            "e2e": None,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak32.value if peak32.value else None, "traffic": None,
+                         "kernel": "Barnes-Hut walk, one rank's share of the targets (slowest rank)",
+                         "peak_source": "ov_measure_fma_peak: FP32 FMA burst on this GPU, this run"},
+            "independent_tangles": indep,
+            "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
         }))
@@ -695,7 +919,7 @@ def main():
         from openvort_b200 import dist as D
         D.close(dist)
         return
-    if args.shard:
+    if args.shard or (world > 1 and not args.independent):
         run_sharded(args, world, rank, local, dist)
         return
 
@@ -800,6 +1024,8 @@ def main():
         err["vs_rel_err_bh_fp64_vs_direct_4096"] = rel(bh64, direct)
         err["vs_rel_err_bh_mixed_vs_direct_4096"] = rel(bhmx, direct)
         err["vs_rel_err_bh_mixed_vs_bh_fp64_4096"] = rel(bhmx, bh64)
+        if world == 1 and not args.no_cpu_baseline:
+            err["bh_vs_direct_reference_4096"] = bh_reference_check(tangle, p, idx, bh64, direct, vs64)
 
     # ---------------- end to end through the reference-named C ABI, pinned
     # host buffers: update_tangle + rk4_step copy in and out every call
@@ -827,12 +1053,14 @@ def main():
                "path": "update_tangents_normals + update_velocities + rk4_step over struct tangle_state "
                        "in pinned host memory"}
 
-    direct = batch = adjoint = reconnection = remeshing = frames = theta_alt = None
+    direct = batch = adjoint = reconnection = remeshing = frames = theta_alt = cfg1 = cfg2 = None
     # the single-GPU objects (and their CPU reference samples) belong to the
     # 1-GPU line; a multi-GPU run measures the headline path only
     if not args.no_extra and world == 1:
         theta_alt = bench_theta(args, ov, tangle, 0.3 if args.theta != 0.3 else 0.5)
         direct = bench_direct(args, ov, peak32.value, peak64.value)
+        cfg2 = bench_cfg2(args, ov)
+        cfg1 = bench_cfg1(args, ov)
         batch = bench_batch(args, ov, peak32.value)
         adjoint = bench_adjoint(args, ov)
         reconnection = bench_reconnect(args, ov, tangle, p)
@@ -852,13 +1080,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
-            "config": {"workload": f"large periodic tangle: {n} points per GPU ({n_rings} rings, D=0.4 cm, "
-                                   f"dl=D/800, radii U[0.02,0.05]D), 26 periodic images, Barnes-Hut "
-                                   f"theta={args.theta}, mixed FP32/FP64, RK4 dt={args.dt}",
-                       "points": n, "points_all_ranks": n_job, "theta": args.theta, "images": 26,
-                       "dt": args.dt,
-                       "parallelism": f"{world} independent tangles (one per GPU)" if world > 1 else "1 GPU",
-                       "l2": "working set (octree cells + node table) larger than the 126 MB L2"},
+            "config": bench_config(args, n, n_job, n_rings, world),
             "rk4_steps_per_s": world * 1e3 / ms_step,
             "fp64": {"value": value64, "ms_per_step": ms64, "rk4_steps_per_s": world * 1e3 / ms64,
                      "roofline_frac_of_fp64_peak": ach64 / peak64.value if peak64.value else None,
@@ -881,6 +1103,8 @@ def main():
                          "tree_build_share_of_step": build_share},
             "other_theta": theta_alt,
             "direct_22k": direct,
+            "cfg2_22k": cfg2,
+            "cfg1_ring": cfg1,
             "batch_4096": batch,
             "adjoint_4096": adjoint,
             "reconnection_1m": reconnection,

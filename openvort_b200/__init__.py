@@ -102,6 +102,10 @@ class DeviceState:
     def download(self, what: int = OV_FIELD_ALL):
         self._rc(self.lib.ov_state_download(self.h, self.t.ptr(), what))
 
+    def upload(self):
+        """Copy the host tangle (positions, links, status, vels) in again."""
+        self._rc(self.lib.ov_state_upload(self.h, self.t.ptr()))
+
     # one tangle over several ranks (ov_state_shard*); openvort_b200.shard
     # drives these with the exchange between begin and end
     def shard_bytes(self, world: int) -> int:

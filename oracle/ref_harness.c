@@ -180,7 +180,7 @@ void refh_sample_eval(struct tangle_state *t, double time, const int *idx, int m
   int i;
 #pragma omp parallel private(i) num_threads(global_num_threads)
   {
-#pragma omp for schedule(dynamic, 4)
+#pragma omp for
     for (i = 0; i < m; ++i) update_velocity(t, idx[i], time, tree);
   }
   double d = now_s();
@@ -188,4 +188,29 @@ void refh_sample_eval(struct tangle_state *t, double time, const int *idx, int m
   *t_geom = b - a;
   *t_build = c - b;
   *t_nodes = d - c;
+}
+
+/* The reference's superfluid velocity vs (src/tangle.c:583-637: local term,
+ * external flow, Biot-Savart sum and image sum) at the m listed nodes, with
+ * its own octree when use_tree (built here, global_BH_resolution) or its
+ * direct sum otherwise; dxi, tangents and normals must be current.  Writes
+ * 3 m doubles.  Returns the seconds of the tree build in *t_build. */
+void refh_sample_vs(struct tangle_state *t, double time, const int *idx, int m, int use_tree,
+                    double *out, double *t_build) {
+  const int keep = global_use_BH;
+  global_use_BH = use_tree;
+  double a = now_s();
+  struct octree *tree = use_tree ? octree_build(t, global_BH_quadtree) : NULL;
+  *t_build = now_s() - a;
+  int i;
+#pragma omp parallel private(i) num_threads(global_num_threads)
+  {
+#pragma omp for
+    for (i = 0; i < m; ++i) {
+      update_velocity(t, idx[i], time, tree);
+      for (int c = 0; c < 3; ++c) out[3 * i + c] = t->vs[idx[i]].p[c];
+    }
+  }
+  if (tree) octree_destroy(tree);
+  global_use_BH = keep;
 }

@@ -6,6 +6,7 @@ from pathlib import Path
 
 import numpy as np
 
+from openvort_b200 import geometry as G
 from openvort_b200.tangle import Flow, HostTangle, Params
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
@@ -57,3 +58,31 @@ def fixture_flows(meta: dict):
     """(index, Flow) of each flow recorded in a flows fixture."""
     return [(i, Flow(f["name"], {n: (tuple(v) if isinstance(v, list) else v) for n, v in f["params"].items()}))
             for i, f in enumerate(meta["flows"])]
+
+
+# The config-2 workload's tangle (512 rings in a periodic cube D = 0.1 cm,
+# radii U[0.02, 0.05] D, dl = D/200, 26 images: 22,379 points), rebuilt from
+# its seed; samples/cfg2_bh4.npz holds the reference's velocities at seeded
+# sample nodes of it and a checksum of its positions.
+CFG2 = {"seed": 2026, "rings": 512, "D": 0.1, "dl": 0.1 / 200, "samples": 256}
+
+
+def cfg2_params(use_bh: int) -> Params:
+    return Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=2 * CFG2["dl"],
+                  hyperfriction=1, use_bh=use_bh, bh_theta=0.4, bh_grain=1e-8,
+                  vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}), vs=Flow("no flow"))
+
+
+def cfg2_tangle():
+    return G.random_ring_tangle(CFG2["seed"], CFG2["rings"], CFG2["D"], dl=CFG2["dl"], boundary="periodic-26")
+
+
+def load_cfg2_samples():
+    """(tangle, sample fixture); asserts the regenerated tangle is the one
+    the reference ran on."""
+    z = np.load(GOLDEN / "samples" / "cfg2_bh4.npz")
+    meta = json.loads(str(z["meta"]))
+    t = cfg2_tangle()
+    assert t.n == meta["n"] and float(np.sum(t.pos)) == meta["pos_sum"] and \
+        float(np.sum(np.abs(t.pos))) == meta["pos_abs_sum"], "generator no longer reproduces the tangle"
+    return t, z

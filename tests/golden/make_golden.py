@@ -4,11 +4,17 @@ own sources by oracle/Makefile).
 
     python tests/golden/make_golden.py
 
-Each fixture holds a seeded input tangle (positions, links, status, box,
-boundary name), the run-time parameters, and the reference's outputs:
+Each fixture in tests/golden/*.npz holds a seeded input tangle (positions,
+links, status, box, boundary name), the run-time parameters, and the
+reference's outputs:
 dxi, tangents, normals, vels, vs after update_tangle, and for the RK4 cases
 the positions after a number of rk4_step calls (update_tangle before each,
-as the reference's main loop does, src/main.c:112-114).
+as the reference's main loop does, src/main.c:112-114).  flows16.npz runs
+every flow of the reference's table; samples/cfg2_bh4.npz holds the
+reference's velocities at sample nodes of a tangle the tests regenerate
+from its seed.
+
+    python tests/golden/make_golden.py [fixture ...]
 """
 from __future__ import annotations
 
@@ -26,6 +32,9 @@ sys.path.insert(0, str(ROOT))
 from openvort_b200 import geometry as G  # noqa: E402
 from openvort_b200.tangle import Flow, Params  # noqa: E402
 from oracle.oracle import Ref, build  # noqa: E402
+
+sys.path.insert(0, str(ROOT / "tests"))
+from cases import CFG2, cfg2_params, cfg2_tangle  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
@@ -125,12 +134,45 @@ def flows16(ref):
     print("flows16", t.n, "nodes")
 
 
+def cfg2_samples(ref):
+    """The 22.4k-point periodic tangle of the config-2 workload (regenerated
+    by the tests from its seed; a checksum pins it): the reference's vs
+    (update_velocity: local term, flow, Biot-Savart, 26 images) at seeded
+    sample nodes with its octree at theta 0.4 and with its direct sum."""
+    import ctypes as C
+    t = cfg2_tangle()
+    rng = np.random.default_rng(CFG2["seed"])
+    idx = np.sort(rng.choice(np.nonzero(t.active)[0], size=CFG2["samples"], replace=False)).astype(np.int32)
+    out = {}
+    for name, use_bh in (("vs_bh4", 1), ("vs_direct", 0)):
+        p = cfg2_params(use_bh)
+        ref.configure(p)
+        tt = t.copy()
+        tt.set_images_from_library(ref.lib)
+        ref.lib.update_tangents_normals.restype = None
+        ref.lib.update_tangents_normals(C.cast(tt.ptr(), C.c_void_p))
+        f = ref.lib.refh_sample_vs
+        f.restype = None
+        f.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                      C.POINTER(C.c_double)]
+        v = np.zeros((len(idx), 3))
+        tb = C.c_double()
+        f(C.cast(tt.ptr(), C.c_void_p), 0.0, idx.ctypes.data, len(idx), use_bh, v.ctypes.data, C.byref(tb))
+        out[name] = v
+    meta = {**CFG2, "n": t.n, "pos_sum": float(np.sum(t.pos)), "pos_abs_sum": float(np.sum(np.abs(t.pos)))}
+    (OUT / "samples").mkdir(exist_ok=True)
+    np.savez_compressed(OUT / "samples" / "cfg2_bh4.npz", meta=np.array(json.dumps(meta)), idx=idx, **out)
+    print("cfg2_bh4 samples", t.n, "nodes")
+
+
 def main():
     build()
     ref = Ref(threads=8)
     only = sys.argv[1:]
     if not only or "flows16" in only:
         flows16(ref)
+    if not only or "cfg2_bh4" in only:
+        cfg2_samples(ref)
     for name, t, p, opt in cases():
         if only and name not in only:
             continue

@@ -113,6 +113,21 @@ def test_spherical_and_simple_is_the_sum_of_its_parts(ov, which):
     assert rel_err(out.vels, want, act) < TOL_V64
 
 
+def test_config2_tangle_bh4_and_direct_vs_reference(ov):
+    """The 22.4k-point periodic tangle of the config-2 workload: FP64
+    Barnes-Hut (theta 0.4) and direct sums against the reference's
+    update_velocity at 256 sample nodes, and the mixed form within its
+    tolerance of the same."""
+    from cases import cfg2_params, load_cfg2_samples
+    t, z = load_cfg2_samples()
+    idx = z["idx"]
+    for use_bh, key in ((1, "vs_bh4"), (0, "vs_direct")):
+        out = gpu_update(ov, t, cfg2_params(use_bh))
+        assert rel_err(out.vs[idx], z[key]) < TOL_V64, key
+        mixed = gpu_update(ov, t, cfg2_params(use_bh), precision=1)
+        assert rel_err(mixed.vs[idx], z[key]) < TOL_MIXED, key
+
+
 def test_device_state_run_vs_oracle(ov, oracle):
     """ov_state_run (device-resident update_tangle + rk4_step) against the
     oracle stepping the same tangle on the CPU."""

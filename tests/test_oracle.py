@@ -49,6 +49,17 @@ def test_oracle_rk4_matches_golden(oracle, name):
         assert pos_err(cur.pos, z[f"rk4_pos_{s + 1}"], t.active) < 1e-14
 
 
+def test_oracle_bh4_on_the_config2_tangle(oracle):
+    """Barnes-Hut theta 0.4 on the 22.4k-point periodic tangle: the restated
+    tree against the reference's update_velocity at 256 sample nodes."""
+    from cases import cfg2_params, load_cfg2_samples
+    t, z = load_cfg2_samples()
+    out = oracle.update_tangle(t, cfg2_params(1))
+    assert rel_err(out.vs[z["idx"]], z["vs_bh4"]) < TOL_V
+    # the tree's approximation is far above the parity bound: the tree ran
+    assert rel_err(z["vs_bh4"], z["vs_direct"]) > 1e-4
+
+
 def test_bh_differs_from_direct(oracle):
     """The Barnes-Hut fixtures exercise the tree: their error against the
     direct sum is the reference's BH error, orders above the parity bound."""
