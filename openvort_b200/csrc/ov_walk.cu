@@ -1086,7 +1086,7 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
   if (multi) {
     int warps = (n_t + 31) / 32;
     int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
-    static const int pair_form = getenv("OV_WALK_PAIR") ? atoi(getenv("OV_WALK_PAIR")) : 1;
+    static const int pair_form = getenv("OV_WALK_PAIR") ? atoi(getenv("OV_WALK_PAIR")) : 0;
     if (mixed && pair_form) {
       const int pwarps = (n_t + 63) / 64;
       const int pblocks = (pwarps + kPairWarps - 1) / kPairWarps;
