@@ -549,6 +549,13 @@ int ov_load_frame(const char *filename, struct tangle_state *tangle, double *tim
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);
 
+/* Accuracy of the FP64 reciprocal square root and reciprocal the direct
+ * sum uses in place of IEEE sqrt and division (hardware approximation plus
+ * two Newton-Raphson steps): the largest differences from 1/sqrt(x) and
+ * 1/x computed with IEEE operations on the device, in ulps, over
+ * x = 2^(e/64), e in [-8192, 8192).  No counterpart in the reference. */
+int ov_check_fast_math(double *rsqrt_ulps, double *rcp_ulps);
+
 #ifdef __cplusplus
 }
 #endif

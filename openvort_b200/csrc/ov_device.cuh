@@ -148,6 +148,53 @@ __device__ __forceinline__ d3 seg_vel64(double f4pi, d3 r1, d3 r2, d3 r) {
   return cross3(R, Rp) * s;
 }
 
+// 1/sqrt(x) and 1/x in FP64 from the hardware approximations
+// (rsqrt.approx.f64, rcp.approx.ftz.f64, relative error ~2^-22) refined by
+// two Newton-Raphson steps each, which square the relative error per step:
+//   1/sqrt(x):  y <- y + y (1 - x y^2) / 2
+//   1/x:        y <- y + y (1 - x y)
+// The results are within a few ulps of the correctly rounded values
+// (ov_check_fast_math measures this on the device); positive normal x only.
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.f64 %0, %1;" : "=d"(y) : "d"(x));
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double r = fma(-(x * y), y, 1.0);
+    y = fma(0.5 * y, r, y);
+  }
+  return y;
+}
+__device__ __forceinline__ double rcp_nr(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+#pragma unroll
+  for (int i = 0; i < 2; ++i) {
+    const double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+  }
+  return y;
+}
+
+// The reference's segment formula without IEEE square roots and divisions:
+// with u = 1/(|R||R'|) from two refined reciprocal square roots,
+//   f (|R| + |R'|) / (|R||R'| (|R||R'| + R.R')) = f (1/|R| + 1/|R'|) u / (1 + R.R' u).
+// R' = R + d (d = r2 - r1, staged per segment) differs from r2 - r by an ulp
+// of |R'|.  Where either cut-off could decide (|R| or |R'| within 1.5x of
+// 1e-8, or cos within 2e-8 of 1) the reference's own operations decide
+// (seg_vel64), so every cut-off decision is the reference's.
+__device__ __forceinline__ d3 seg_vel64_nr(double f4pi, d3 r1, d3 r2, d3 d, d3 r) {
+  const d3 R = r1 - r;
+  const d3 Rp = R + d;
+  const double R2 = dot3(R, R), Rp2 = dot3(Rp, Rp), RRp = dot3(R, Rp);
+  if (R2 < 2.25e-16 || Rp2 < 2.25e-16) return seg_vel64(f4pi, r1, r2, r);
+  const double ia = rsqrt_nr(R2), ib = rsqrt_nr(Rp2);
+  const double u = ia * ib;
+  if (fabs(fma(RRp, u, -1.0)) < 2e-8) return seg_vel64(f4pi, r1, r2, r);
+  const double s = f4pi * (ia + ib) * (u * rcp_nr(fma(RRp, u, 1.0)));
+  return cross3(R, Rp) * s;
+}
+
 // FP32 far-field form: R and the segment vector ds are formed in FP64 by the
 // caller and rounded once; R x R' = R x ds avoids the cancellation of the
 // product of two nearly parallel long vectors.  Only used where |R| >= 4|ds|,

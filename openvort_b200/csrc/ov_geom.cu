@@ -112,9 +112,10 @@ __global__ void k_epilogue(OvParams P, Links L, const double* __restrict__ t_dev
                            const double* __restrict__ pos, const double* __restrict__ tan,
                            const double* __restrict__ nrm, const double* __restrict__ v_nl,
                            const double* __restrict__ v_img, double* vels, double* vs_out, int k0,
-                           int k1, int* flag) {
-  int k = k0 + blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= k1) return;
+                           int k1, const int* __restrict__ idx, int* flag) {
+  const int i = k0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= k1) return;
+  const int k = idx ? idx[i] : i;
   const double t = t_dev ? t0 + *t_dev : t0;
   int2 st = L.st[k];
   if (st.x == OV_EMPTY) return;
@@ -220,7 +221,20 @@ bool ov_launch_epilogue(cudaStream_t st, const OvParams& P, const int2* links, c
   if (k1 <= k0) return true;
   Links L{links, status};
   k_epilogue<<<blocks_for(k1 - k0), kThreads, 0, st>>>(P, L, t_dev, t0, pos, tan, nrm, v_nl, v_img,
-                                                         vels, vs, k0, k1, flag);
+                                                         vels, vs, k0, k1, nullptr, flag);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_launch_epilogue_list(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                             double t0, const double* pos, const double* tan, const double* nrm,
+                             const double* v_nl, const double* v_img, double* vels, double* vs,
+                             const int* idx, int count, int* flag) {
+  if (count <= 0) return true;
+  Links L{links, status};
+  k_epilogue<<<blocks_for(count), kThreads, 0, st>>>(P, L, nullptr, t0, pos, tan, nrm, v_nl, v_img, vels,
+                                                     vs, 0, count, idx, flag);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   return true;

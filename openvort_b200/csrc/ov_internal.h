@@ -215,6 +215,11 @@ bool ov_launch_epilogue(cudaStream_t st, const OvParams& P, const int2* links, c
                         const double* t_dev, double t0, const double* pos, const double* tan,
                         const double* nrm, const double* v_nl, const double* v_img, double* vels,
                         double* vs, int k0, int k1, int* flag);
+// the epilogue of the slots idx[0 .. count-1] at time t0
+bool ov_launch_epilogue_list(cudaStream_t st, const OvParams& P, const int2* links, const int2* status,
+                             double t0, const double* pos, const double* tan, const double* nrm,
+                             const double* v_nl, const double* v_img, double* vels, double* vs,
+                             const int* idx, int count, int* flag);
 bool ov_launch_euler(cudaStream_t st, const int2* status, const double* x0, const double* v,
                      double h, double* xs, int n);
 bool ov_launch_rk4_combine(cudaStream_t st, const int2* status, const double* k1, const double* k2,

@@ -1,9 +1,19 @@
 // ov_peak.cu - FMA throughput microbenchmark: the FP32 / FP64 roofline
-// denominators of the Biot-Savart kernels, measured on the running GPU.
+// denominators of the Biot-Savart kernels, measured on the running GPU; and
+// the accuracy check of the refined FP64 reciprocal square root and
+// reciprocal the direct sum uses.
 // Eight independent FMA chains per thread keep the pipes full; the result is
 // written so the chains are not eliminated.
+#include <string.h>
+
 #include "openvort_b200.h"
 #include "ov_internal.h"
+
+static double __longlong_as_double_host(unsigned long long v) {
+  double d;
+  memcpy(&d, &v, sizeof(d));
+  return d;
+}
 
 namespace {
 
@@ -56,7 +66,43 @@ bool run(double* tflops) {
   return true;
 }
 
+// refined reciprocal square root and reciprocal (rsqrt_nr, rcp_nr) against
+// IEEE sqrt and division, over x = 2^(e / 64) for e in [-8192, 8192): the
+// largest relative differences, in ulps of the IEEE result (atomicMax on the
+// bit patterns of non-negative doubles orders them as numbers)
+__global__ void k_check_fast_math(unsigned long long* worst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 16384) return;
+  const double x = exp2((i - 8192) / 64.0);
+  const double a = 1.0 / sqrt(x), b = rsqrt_nr(x);
+  const double c = 1.0 / x, d = rcp_nr(x);
+  const double ulp_a = a * 0x1p-52, ulp_c = c * 0x1p-52;
+  atomicMax(&worst[0], (unsigned long long)__double_as_longlong(fabs(b - a) / ulp_a));
+  atomicMax(&worst[1], (unsigned long long)__double_as_longlong(fabs(d - c) / ulp_c));
+}
+
 }  // namespace
+
+extern "C" int ov_check_fast_math(double* rsqrt_ulps, double* rcp_ulps) {
+  ov_clear_error();
+  if (!rsqrt_ulps || !rcp_ulps) return OV_ERR_INVALID;
+  if (ov_init(0) != OV_OK) return ov_last_error();
+  unsigned long long* d = nullptr;
+  unsigned long long h[2] = {0, 0};
+  if (!ov_cuda_ok(cudaMalloc(&d, sizeof(h)), "cudaMalloc")) return ov_last_error();
+  bool ok = ov_cuda_ok(cudaMemset(d, 0, sizeof(h)), "cudaMemset");
+  if (ok) {
+    k_check_fast_math<<<64, 256>>>(d);
+    OV_LAUNCHED();
+    ok = ov_cuda_ok(cudaGetLastError(), "k_check_fast_math") &&
+         ov_cuda_ok(cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost), "cudaMemcpy");
+  }
+  cudaFree(d);
+  if (!ok) return ov_last_error();
+  *rsqrt_ulps = __longlong_as_double_host(h[0]);
+  *rcp_ulps = __longlong_as_double_host(h[1]);
+  return OV_OK;
+}
 
 extern "C" int ov_measure_fma_peak(int fp64, double* tflops) {
   ov_clear_error();

@@ -138,93 +138,79 @@ __global__ void k_rec_scan(OvParams P, Grid g, const double* __restrict__ pos, c
 }
 
 // ---------------------------------------------------------------- velocities
-// The nonlocal and image sums (update_velocity's loops, src/tangle.c:611-636)
-// at the two nodes of a candidate pair, spread over the whole GPU: block
-// (c, j) sums segments [c chunk, (c + 1) chunk) at image j of both nodes,
-// reduced in a fixed order in shared memory; k_pair_reduce then adds the
-// blocks in order.
-constexpr int kPV = 256;
+// The approach test needs update_velocity (src/tangle.c:583-684) of both
+// nodes on the links current at the test.  Velocities of the nodes of the
+// next candidates come from one batched FP64 direct sum over all segments
+// and images (ov_direct_points); after each reconnection every node computed
+// so far gets the exact change: the two removed and the two added segments
+// of do_reconnection over the tangle and all its images.  A node's epilogue
+// (local term, flows, friction) then follows on the current links.
 
-struct SegRef {
-  const double* r1r2;   // 6 doubles per slot: r1, wrapped r2 (k_segtab)
-  const int* fwd;
+// targets of a batch: node positions, each skipping its own segments
+__global__ void k_rec_points(const int* __restrict__ nodes, int count, const double* __restrict__ pos,
+                             double* pts, int* skip) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int k = nodes[i];
+  st3(pts, i, ld3(pos, k));
+  skip[i] = k;
+}
+
+__global__ void k_rec_scatter(const int* __restrict__ nodes, int count, const double* __restrict__ nl,
+                              const double* __restrict__ img, double* v_nl, double* v_img) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int k = nodes[i];
+  st3(v_nl, k, ld3(nl, i));
+  st3(v_img, k, ld3(img, i));
+}
+
+// one segment change of a reconnection: slot m's forward link was (sign -1)
+// or is now (sign +1) f
+struct SegChange {
+  int m[4], f[4];
+  double sign[4];
 };
 
-__global__ void __launch_bounds__(kPV) k_pair_vel(OvParams P, SegRef S, int n, const double* __restrict__ pos,
-                                                  int2 tk, int chunk, double* __restrict__ partial) {
-  __shared__ double red[kPV][6];
-  const int c = blockIdx.x, j = blockIdx.y, nch = gridDim.x;
-  d3 r[2];
-  int skip[2];
-  const int t2[2] = {tk.x, tk.y};
-#pragma unroll
-  for (int u = 0; u < 2; ++u) {
-    r[u] = ld3(pos, t2[u]);
-    skip[u] = -1;
-    if (j > 0) r[u] = image_point(P, j - 1, r[u]);
-    else skip[u] = t2[u];
-  }
-  double a[6] = {0, 0, 0, 0, 0, 0};
-  const int hi = min(n, (c + 1) * chunk);
-  for (int m = c * chunk + threadIdx.x; m < hi; m += kPV) {
-    const int fw = S.fwd[m];
-    if (fw < 0) continue;
-    const double* sg = S.r1r2 + 6 * (size_t)m;
-    const d3 r1 = mk3(sg[0], sg[1], sg[2]), r2 = mk3(sg[3], sg[4], sg[5]);
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      if (m == skip[u] || fw == skip[u]) continue;
-      const d3 v = seg_vel64(P.f4pi, r1, r2, r[u]);
-      a[3 * u] += v.x;
-      a[3 * u + 1] += v.y;
-      a[3 * u + 2] += v.z;
+// v_nl and v_img of the listed nodes += the changed segments' fields, with
+// the skip rule of the tangle's own sum (src/tangle.c:614-616) and the
+// mirror reflection of each image's sum (src/tangle.c:633-634)
+__global__ void k_rec_correct(OvParams P, SegChange C, const int* __restrict__ nodes, int count,
+                              const double* __restrict__ pos, double* v_nl, double* v_img) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int k = nodes[i];
+  const d3 r = ld3(pos, k);
+  d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
+  for (int c = 0; c < 4; ++c) {
+    const d3 r1 = ld3(pos, C.m[c]);
+    const d3 r2 = pwrap(P, r1, ld3(pos, C.f[c]));
+    if (k != C.m[c] && k != C.f[c]) nl = nl + seg_vel64(P.f4pi, r1, r2, r) * C.sign[c];
+    for (int j = 0; j < P.n_img; ++j) {
+      d3 v = seg_vel64(P.f4pi, r1, r2, image_point(P, j, r)) * C.sign[c];
+      const int face = P.img[j][3];
+      if (face > -1) v = mirror_dir(v, face);
+      im = im + v;
     }
   }
-#pragma unroll
-  for (int q = 0; q < 6; ++q) red[threadIdx.x][q] = a[q];
-  __syncthreads();
-  for (int s = kPV / 2; s > 0; s >>= 1) {
-    if (threadIdx.x < s)
-      for (int q = 0; q < 6; ++q) red[threadIdx.x][q] += red[threadIdx.x + s][q];
-    __syncthreads();
-  }
-  if (threadIdx.x < 6) partial[((size_t)j * nch + c) * 6 + threadIdx.x] = red[0][threadIdx.x];
+  st3(v_nl, k, ld3(v_nl, k) + nl);
+  st3(v_img, k, ld3(v_img, k) + im);
 }
 
-// v_nl and v_img of both nodes from the blocks' partial sums, in order;
-// mirror images reflect their velocity (src/tangle.c:633-634)
-__global__ void k_pair_reduce(OvParams P, const double* __restrict__ partial, int nch, int2 tk,
-                              double* v_nl, double* v_img) {
-  const int u = threadIdx.x;
-  if (u >= 2) return;
-  d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
-  for (int c = 0; c < nch; ++c) nl = nl + ld3(partial + (size_t)c * 6, u);
-  for (int j = 1; j <= P.n_img; ++j) {
-    d3 v = mk3(0, 0, 0);
-    for (int c = 0; c < nch; ++c) v = v + ld3(partial + ((size_t)j * nch + c) * 6, u);
-    const int face = P.img[j - 1][3];
-    if (face > -1) v = mirror_dir(v, face);
-    im = im + v;
-  }
-  const int k = u == 0 ? tk.x : tk.y;
-  st3(v_nl, k, nl);
-  st3(v_img, k, im);
-}
-
-// vels and vs of nodes k and l and the status flag, packed for one copy
-__global__ void k_pair_pack(const double* __restrict__ vels, const double* __restrict__ vs, int2 tk,
-                            const int* __restrict__ flag, double* out) {
-  const int i = threadIdx.x;
-  if (i < 12) {
-    const int node = i < 6 ? tk.x : tk.y, c = i % 3;
-    out[i] = (i % 6 < 3 ? vels : vs)[3 * (size_t)node + c];
-  }
-  if (i == 12) out[12] = (double)*flag;
+// vels and vs of the listed nodes, packed 6 doubles per node for one copy
+__global__ void k_rec_pack(const int* __restrict__ nodes, int count, const double* __restrict__ vels,
+                           const double* __restrict__ vs, double* out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const int k = nodes[i];
+  st3(out + 6 * (size_t)i, 0, ld3(vels, k));
+  st3(out + 6 * (size_t)i + 3, 0, ld3(vs, k));
 }
 
 struct RecState {
   ov_state_impl s;
-  DevBuf keys, keys2, ids, ids2, pairs, count, tmp, skip, partial, pack;
+  DevBuf keys, keys2, ids, ids2, pairs, count, tmp, skip, pack;
+  DevBuf batch, pts, bnl, bimg, known;   // batched velocities
 };
 
 RecState& rec_state() {
@@ -362,59 +348,75 @@ bool upload_for_pass(RecState& R, const tangle_state* t) {
   return true;
 }
 
-// update_velocity (src/tangle.c:583-684) of nodes k and l on the resident
-// state (direct sum: the reference passes no tree here), written back to
-// the tangle's vels and vs
-bool pair_velocity(RecState& R, tangle_state* t, int k, int l, double time) {
+// Velocities (vels, vs) of the nodes known so far, as the device holds them
+// on the current links, mirrored on the host: node k's values at
+// hv[6 * pos_of[k]].
+struct RecVel {
+  std::vector<int> known;        // slots with velocities on the device
+  std::vector<int> pos_of;       // slot -> index in known, -1 if not known
+  std::vector<double> hv;        // 6 per known node: vels, vs
+  double time = 0;
+};
+
+// epilogue of every known node and the copy of their vels and vs to the host
+bool refresh_known(RecState& R, RecVel& V) {
   ov_state_impl* s = &R.s;
-  const int n = s->n;
-  const int2 tk = make_int2(k, l);
+  const int cnt = (int)V.known.size();
+  if (cnt == 0) return true;
+  int* flag = s->dflag.as<int>();
+  OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
+  if (!ov_launch_epilogue_list(s->stream, s->P, s->links.as<int2>(), s->status.as<int2>(), V.time,
+                               s->pos.as<double>(), s->tan.as<double>(), s->nrm.as<double>(),
+                               s->v_nl.as<double>(), s->v_img.as<double>(), s->vels.as<double>(),
+                               s->vs.as<double>(), R.known.as<int>(), cnt, flag))
+    return false;
+  if (!R.pack.reserve(sizeof(double) * 6 * (size_t)cnt + 64)) return false;
+  k_rec_pack<<<(cnt + 255) / 256, 256, 0, s->stream>>>(R.known.as<int>(), cnt, s->vels.as<double>(),
+                                                       s->vs.as<double>(), R.pack.as<double>());
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  int h_flag = 0;
+  V.hv.resize(6 * (size_t)cnt);
+  OV_TRY_CUDA(cudaMemcpyAsync(V.hv.data(), R.pack.p, sizeof(double) * 6 * (size_t)cnt, cudaMemcpyDeviceToHost,
+                              s->stream));
+  OV_TRY_CUDA(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  return ov_flag_status(h_flag, "update_velocity");
+}
+
+// Nonlocal and image sums of new nodes on the current links (one batched
+// FP64 direct sum), added to the known set; then every known node's
+// epilogue and host copy.
+bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes) {
+  ov_state_impl* s = &R.s;
+  const int m = (int)nodes.size();
+  if (m == 0) return true;
+  const int old = (int)V.known.size();
+  for (int k : nodes) {
+    V.pos_of[k] = (int)V.known.size();
+    V.known.push_back(k);
+  }
+  const int cnt = (int)V.known.size();
+  if (!R.known.reserve(sizeof(int) * (size_t)cnt) || !R.pts.reserve(sizeof(double) * 3 * (size_t)m) ||
+      !R.skip.reserve(sizeof(int) * (size_t)m) || !R.bnl.reserve(sizeof(double) * 3 * (size_t)m) ||
+      !R.bimg.reserve(sizeof(double) * 3 * (size_t)m))
+    return false;
+  OV_TRY_CUDA(cudaMemcpyAsync(R.known.as<int>() + old, V.known.data() + old, sizeof(int) * (size_t)m,
+                              cudaMemcpyHostToDevice, s->stream));
+  const int* batch = R.known.as<int>() + old;
   if (!s->P.lia_only) {
-    // segment table of the current links
-    if (!ov_segment_table(s, s->pos.as<double>())) return false;
-    const int nimg = s->P.n_img;
-    static int sms = 0;
-    if (!sms) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 1;
-    }
-    // about 8 blocks of 256 threads per SM: the FP64 sum is latency-bound
-    const int want = std::max(1, (8 * sms + nimg) / (nimg + 1));
-    const int chunk = std::max(kPV, (n + want - 1) / want);
-    const int nch = (n + chunk - 1) / chunk;
-    if (!R.partial.reserve(sizeof(double) * 6 * (size_t)nch * (nimg + 1))) return false;
-    k_pair_vel<<<dim3(nch, nimg + 1), kPV, 0, s->stream>>>(s->P, SegRef{s->seg64.as<double>(), s->segid.as<int>()},
-                                                           n, s->pos.as<double>(), tk, chunk, R.partial.as<double>());
+    k_rec_points<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->pos.as<double>(), R.pts.as<double>(),
+                                                          R.skip.as<int>());
     OV_LAUNCHED();
-    k_pair_reduce<<<1, 32, 0, s->stream>>>(s->P, R.partial.as<double>(), nch, tk, s->v_nl.as<double>(),
-                                           s->v_img.as<double>());
+    if (!ov_direct_points(s, s->pos.as<double>(), m, R.pts.as<double>(), R.skip.as<int>(), nullptr, 0,
+                          R.bnl.as<double>(), R.bimg.as<double>()))
+      return false;
+    k_rec_scatter<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, R.bnl.as<double>(), R.bimg.as<double>(),
+                                                           s->v_nl.as<double>(), s->v_img.as<double>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
   }
-  int* flag = s->dflag.as<int>();
-  OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
-  for (int u = 0; u < 2; ++u) {
-    const int m = u == 0 ? k : l;
-    if (!ov_launch_epilogue(s->stream, s->P, s->links.as<int2>(), s->status.as<int2>(), nullptr, time,
-                            s->pos.as<double>(), s->tan.as<double>(), s->nrm.as<double>(), s->v_nl.as<double>(),
-                            s->v_img.as<double>(), s->vels.as<double>(), s->vs.as<double>(), m, m + 1, flag))
-      return false;
-  }
-  if (!R.pack.reserve(sizeof(double) * 13)) return false;
-  k_pair_pack<<<1, 32, 0, s->stream>>>(s->vels.as<double>(), s->vs.as<double>(), tk, flag, R.pack.as<double>());
-  OV_LAUNCHED();
-  OV_TRY_CUDA(cudaGetLastError());
-  double h[13];
-  OV_TRY_CUDA(cudaMemcpyAsync(h, R.pack.p, sizeof(h), cudaMemcpyDeviceToHost, s->stream));
-  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
-  for (int c = 0; c < 3; ++c) {
-    t->vels[k].p[c] = h[c];
-    t->vs[k].p[c] = h[3 + c];
-    t->vels[l].p[c] = h[6 + c];
-    t->vs[l].p[c] = h[9 + c];
-  }
-  return ov_flag_status((int)h[12], "update_velocity");
+  return refresh_known(R, V);
 }
 
 }  // namespace
@@ -449,17 +451,50 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
   std::vector<int2> cand;
   if (!upload_for_pass(R, tangle) || !find_candidates(R, tangle, rec_dist, rec_angle, cand))
     return -ov_last_error();
+  ov_state_impl* s = &R.s;
+  RecVel V;
+  V.pos_of.assign(tangle->N, -1);
+  V.time = t;
+  // the nodes of this many upcoming candidates per batched direct sum
+  constexpr int kBatchNodes = 2048;
   // recalculate holds the sit-out flags on entry: the reference zeroes them
   // at the top of reconnect (src/vortex_dynamics.c:148-149), before its wall
   // part, whose reconnections the loop then leaves alone
+  auto linked = [&](int k, int l) {
+    return tangle->connections[k].forward == l || tangle->connections[k].reverse == l;
+  };
   int nrecs = 0, done_k = -1;
-  for (const int2& pr : cand) {
-    const int k = pr.x, l = pr.y;
+  for (size_t i = 0; i < cand.size(); ++i) {
+    const int k = cand[i].x, l = cand[i].y;
     // after a reconnection the reference leaves k's inner loop
-    if (k == done_k || tangle->recalculate[k] || tangle->recalculate[l]) continue;
-    if (tangle->connections[k].forward == l || tangle->connections[k].reverse == l) continue;
-    // approach test on the current links (src/vortex_dynamics.c:266-277)
-    if (!pair_velocity(R, tangle, k, l, t)) return -ov_last_error();
+    if (k == done_k || tangle->recalculate[k] || tangle->recalculate[l] || linked(k, l)) continue;
+    if (V.pos_of[k] < 0 || V.pos_of[l] < 0) {
+      // velocities of the nodes of the next candidates that can still be
+      // tested (some may be skipped after later reconnections)
+      std::vector<int> batch;
+      for (size_t j = i; j < cand.size() && (int)batch.size() < kBatchNodes; ++j) {
+        const int a = cand[j].x, b = cand[j].y;
+        if (tangle->recalculate[a] || tangle->recalculate[b] || linked(a, b)) continue;
+        for (int x : {a, b})
+          if (V.pos_of[x] == -1) {
+            V.pos_of[x] = -2;   // queued
+            batch.push_back(x);
+          }
+      }
+      for (int x : batch) V.pos_of[x] = -1;
+      if (!compute_nodes(R, V, batch)) return -ov_last_error();
+    }
+    // update_velocity of both nodes writes their vels and vs (as the
+    // reference's does, src/vortex_dynamics.c:275-276)
+    const double* hk = V.hv.data() + 6 * (size_t)V.pos_of[k];
+    const double* hl = V.hv.data() + 6 * (size_t)V.pos_of[l];
+    for (int c = 0; c < 3; ++c) {
+      tangle->vels[k].p[c] = hk[c];
+      tangle->vs[k].p[c] = hk[3 + c];
+      tangle->vels[l].p[c] = hl[c];
+      tangle->vs[l].p[c] = hl[3 + c];
+    }
+    // approach test (src/vortex_dynamics.c:266-281)
     double w[3], dx[3], dv[3];
     h_pwrap(tangle, tangle->vnodes[k].p, tangle->vnodes[l].p, w);
     for (int c = 0; c < 3; ++c) {
@@ -471,13 +506,17 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     if (dot > 0) continue;
     const int knext = tangle->connections[k].forward, kprev = tangle->connections[k].reverse;
     const int lnext = tangle->connections[l].forward, lprev = tangle->connections[l].reverse;
-    int changed[4];
+    int changed[4], old_fwd[2];
     if (!do_reconnection(tangle, k, l, changed)) continue;
+    // changed[0] and changed[3] are the slots whose forward link changed:
+    // k (was kf) and lr (was l), or l (was lf) and kr (was k)
+    old_fwd[0] = changed[0] == k ? knext : lnext;
+    old_fwd[1] = changed[0] == k ? l : k;
     // the same links on the device
     for (int c = 0; c < 4; ++c) {
       const int m = changed[c];
-      if (!ov_cuda_ok(cudaMemcpyAsync(R.s.links.as<int2>() + m, &tangle->connections[m], sizeof(int2),
-                                      cudaMemcpyHostToDevice, R.s.stream),
+      if (!ov_cuda_ok(cudaMemcpyAsync(s->links.as<int2>() + m, &tangle->connections[m], sizeof(int2),
+                                      cudaMemcpyHostToDevice, s->stream),
                       "cudaMemcpyAsync"))
         return -ov_last_error();
     }
@@ -486,8 +525,22 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     for (int f : flag) tangle->recalculate[f]++;
     ++nrecs;
     done_k = k;
+    // every known node: the removed and added segments' fields
+    SegChange C;
+    C.m[0] = changed[0]; C.f[0] = old_fwd[0]; C.sign[0] = -1;
+    C.m[1] = changed[3]; C.f[1] = old_fwd[1]; C.sign[1] = -1;
+    C.m[2] = changed[0]; C.f[2] = tangle->connections[changed[0]].forward; C.sign[2] = 1;
+    C.m[3] = changed[3]; C.f[3] = tangle->connections[changed[3]].forward; C.sign[3] = 1;
+    const int cnt = (int)V.known.size();
+    if (cnt > 0 && !s->P.lia_only) {
+      k_rec_correct<<<(cnt + 127) / 128, 128, 0, s->stream>>>(s->P, C, R.known.as<int>(), cnt, s->pos.as<double>(),
+                                                               s->v_nl.as<double>(), s->v_img.as<double>());
+      OV_LAUNCHED();
+      if (!ov_cuda_ok(cudaGetLastError(), "k_rec_correct")) return -ov_last_error();
+    }
+    if (!refresh_known(R, V)) return -ov_last_error();
   }
-  if (!ov_cuda_ok(cudaStreamSynchronize(R.s.stream), "cudaStreamSynchronize")) return -ov_last_error();
+  if (!ov_cuda_ok(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize")) return -ov_last_error();
   return nrecs;
 }
 

@@ -29,11 +29,14 @@ REF_SRC = Path(os.environ.get("OPENVORT_REF", "/root/reference"))
 
 
 def build(ref: bool = True):
-    """Compile liboracle.so, and _ref/libov_ref.so when the reference sources
-    are present (this container); elsewhere the prebuilt file is used."""
+    """Compile liboracle.so, and _ref/libov_ref.so with the linked main-loop
+    programs when the reference sources are present; elsewhere the prebuilt
+    files are used."""
     targets = ["liboracle.so"]
     if ref and (REF_SRC / "src" / "tangle.c").exists():
-        targets.append("ref")
+        # the reference library, and its main loop built unmodified and
+        # linked against libov_gpu.so (which must be built first)
+        targets += ["ref", "linked"]
     subprocess.run(["make", "-s", "-C", str(HERE), f"REF={REF_SRC}", *targets], check=True)
 
 

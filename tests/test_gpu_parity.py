@@ -128,6 +128,16 @@ def test_config2_tangle_bh4_and_direct_vs_reference(ov):
         assert rel_err(mixed.vs[idx], z[key]) < TOL_MIXED, key
 
 
+def test_refined_fp64_reciprocals_match_ieee(ov):
+    """The direct sum's FP64 1/sqrt(x) and 1/x (hardware approximation plus
+    two Newton-Raphson steps) stay within 4 ulps of IEEE sqrt and division
+    over 2^-128 .. 2^128."""
+    lib = ov.load()
+    a, b = C.c_double(-1), C.c_double(-1)
+    assert lib.ov_check_fast_math(C.byref(a), C.byref(b)) == 0, lib.ov_last_error_message()
+    assert 0 <= a.value <= 4.0 and 0 <= b.value <= 4.0, (a.value, b.value)
+
+
 def test_device_state_run_vs_oracle(ov, oracle):
     """ov_state_run (device-resident update_tangle + rk4_step) against the
     oracle stepping the same tangle on the CPU."""
