@@ -77,12 +77,15 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the direct-sum and batch lines")
     ap.add_argument("--batch-steps", type=int, default=200)
+    ap.add_argument("--batch-systems", type=int, default=4096)
     ap.add_argument("--cfg1-steps", type=int, default=1000)
     ap.add_argument("--cfg2-steps", type=int, default=500)
     ap.add_argument("--cfg2-direct-steps", type=int, default=20)
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--shard", action="store_true",
                     help="at one GPU too: the sharded one-tangle run (the default when --gpus > 1)")
+    ap.add_argument("--only", choices=["walk", "direct", "batch", "cfg2", "adjoint", "reconnect"],
+                    help="run one part alone and print its object (for profiling)")
     ap.add_argument("--independent", action="store_true",
                     help="with --gpus > 1: one independent tangle per rank (weak scaling) as the headline")
     return ap.parse_args()
@@ -494,7 +497,7 @@ def bench_batch(args, ov, peak32: float):
     step, autotuned kernel shape."""
     from openvort_b200 import geometry as G
     from openvort_b200.tangle import Flow, Params
-    t, off, _ = G.ring_pair_ensemble(args.seed + 4, 4096, n_range=(64, 2048))
+    t, off, _ = G.ring_pair_ensemble(args.seed + 4, args.batch_systems, n_range=(64, 2048))
     p = Params(core_a=1e-8, alpha=0.098, alpha_p=0.016, use_mf=1, dl_max=1e-2, hyperfriction=0,
                use_bh=0, vn=Flow("no flow"), vs=Flow("no flow"))
     # the finest systems (2048 points on r = 5e-3 cm rings, spacing 3e-5 cm)
@@ -502,8 +505,8 @@ def bench_batch(args, ov, peak32: float):
     # dt below ~5e-7 s there
     dt = 2.5e-7
     n = int(t.active.sum())
-    out = {"workload": f"4096 ring-pair systems, {n} points, open boundaries, direct sums per system, "
-                       f"RK4 dt={dt}", "points": n, "systems": 4096, "steps": args.batch_steps}
+    out = {"workload": f"{args.batch_systems} ring-pair systems, {n} points, open boundaries, direct sums per system, "
+                       f"RK4 dt={dt}", "points": n, "systems": args.batch_systems, "steps": args.batch_steps}
     ov.configure(p, ov.OV_PREC_MIXED)
     b = ov.DeviceBatch(t.copy(), off)
     tu = b.autotune()
@@ -932,6 +935,23 @@ def main():
         raise SystemExit(f"libov_gpu: {lib.ov_last_error_message().decode()}")
     torch.cuda.set_device(local)
     p = params(args.theta)
+    if args.only and args.only != "walk":
+        peak32, peak64 = C.c_double(0), C.c_double(0)
+        lib.ov_measure_fma_peak(0, C.byref(peak32))
+        lib.ov_measure_fma_peak(1, C.byref(peak64))
+        part = {"direct": lambda: bench_direct(args, ov, peak32.value, peak64.value),
+                "batch": lambda: bench_batch(args, ov, peak32.value),
+                "cfg2": lambda: bench_cfg2(args, ov),
+                "adjoint": lambda: bench_adjoint(args, ov)}
+        if args.only == "reconnect":
+            t, _ = make_tangle(args.points, args.seed)
+            out = bench_reconnect(args, ov, t, p)
+        else:
+            out = part[args.only]()
+        print(json.dumps({"only": args.only, args.only: out}))
+        from openvort_b200 import dist as D
+        D.close(dist)
+        return
     from openvort_b200.dist import rank_seed
     tangle, n_rings = make_tangle(args.points, rank_seed(args.seed, rank))
     n = int(tangle.active.sum())
@@ -966,6 +986,14 @@ def main():
     walk_share = rs.bs_kernel_ms / ms_run if ms_run > 0 else None
     build_share = rs.build_ms / ms_run if ms_run > 0 else None
     st.close()
+    if args.only == "walk":
+        print(json.dumps({"only": "walk", "points": n, "ms_per_step": ms_step, "walk_ms": walk_ms,
+                          "achieved_tflops": achieved, "peak_tflops": peak32.value,
+                          "frac": achieved / peak32.value if peak32.value else None,
+                          "cell_interactions_per_point": rs.cell_interactions / max(1.0, rs.bs_launches) / n}))
+        from openvort_b200 import dist as D
+        D.close(dist)
+        return
 
     # ---------------- plain FP64 form, same workload
     ov.configure(p, ov.OV_PREC_FP64)

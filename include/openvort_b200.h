@@ -386,9 +386,11 @@ int ov_batch_run(ov_batch *b, double t0, double dt, int nsteps);
 /* copy results of every system out (OV_FIELD_* mask) */
 int ov_batch_download(ov_batch *b, struct tangle_state *all, int what);
 /* Biot-Savart kernel shape: targets per block (64, 128 or 256), sources
- * per shared-memory tile (64, 128 or 256) and resident blocks per SM of the
- * persistent grid (0: as many as fit).  ov_batch_autotune times the
- * candidates on the batch's own systems and keeps the fastest. */
+ * per shared-memory tile (64, 128 or 256; 0: the mixed form in chain order,
+ * whose consecutive segments share end nodes, in tiles of 128) and resident
+ * blocks per SM of the persistent grid (0: as many as fit).
+ * ov_batch_autotune times the candidates on the batch's own systems and
+ * keeps the fastest. */
 typedef struct {
   int targets_per_block;
   int sources_per_tile;

@@ -183,6 +183,149 @@ __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
   }
 }
 
+// Mixed form in chain order (chain_sweep, ov_pair.cuh): each system's
+// segments in slot order, where its rings run slot after slot, so a chained
+// segment shares its end node with the next and each node's offset and
+// 1/|R| serve both; a ring's closing segment takes the two-source form.
+// Two-float offsets from the coordinate origin (the systems span whole
+// rings, and a slot may be EMPTY); near pairs and pairs at the colinearity
+// cut-off in FP64, FP32 partial sums over 32 segments added into FP64 sums.
+template <int TB>
+__global__ void __launch_bounds__(TB) k_batch_bs_chain(OvParams P, BatchView B,
+                                                       const double* __restrict__ pos,
+                                                       const int2* __restrict__ links,
+                                                       const int2* __restrict__ status,
+                                                       double* __restrict__ v_nl,
+                                                       int* __restrict__ work) {
+  __shared__ ChainNode<true> sh_node[kCH + 1];
+  __shared__ ChainSeg sh_seg[kCH];
+  __shared__ PairSrc<true> sh_irr[kCH];
+  __shared__ int sh_irr_id[2 * kCH];
+  __shared__ int sh_item, sh_n_irr;
+  const double f4pi = P.f4pi;
+  const d3 O = mk3(0, 0, 0);
+  for (;;) {
+    __syncthreads();
+    if (threadIdx.x == 0) sh_item = atomicAdd(work, 1);
+    __syncthreads();
+    const int it = sh_item;
+    if (it >= B.n_items) return;
+    const int2 w = B.items[it];
+    const int s0 = B.off[w.x], s1 = B.off[w.x + 1];
+    const double near2 = B.near2[w.x];
+    int kk[kTT];
+    PairTargets T;
+    double acc[kTT][3];
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) {
+      const int k = w.y + threadIdx.x + TB * u;
+      const bool act = k < s1 && status[k].x == OV_FREE;
+      kk[u] = act ? k : -1;
+      const d3 r = act ? ld3(pos, k) : O;
+      set_target(T, u, r.x, r.y, r.z);
+      acc[u][0] = acc[u][1] = acc[u][2] = 0;
+    }
+    auto special = [&](int u, int id) {
+#pragma unroll
+      for (int v = 0; v < kTT; ++v) {
+        if (v != u) continue;
+        const int k = kk[v];
+        if (k < 0 || id < 0) return;
+        const d3 vv = seg_vel64(f4pi, ld3(pos, id), ld3(pos, links[id].x), ld3(pos, k));
+        acc[v][0] += vv.x;
+        acc[v][1] += vv.y;
+        acc[v][2] += vv.z;
+      }
+    };
+    // the segment starting at slot m: forward slot (or -1), vector, far radius
+    auto seg_of = [&](int m, double* d, double* far2) -> int {
+      if (m >= s1 || status[m].x == OV_EMPTY) return -1;
+      const int f = links[m].x;
+      if (f < 0) return -1;
+      const d3 a = ld3(pos, m), bb = ld3(pos, f);
+      d[0] = bb.x - a.x;
+      d[1] = bb.y - a.y;
+      d[2] = bb.z - a.z;
+      *far2 = fmax(16.0 * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]), near2);
+      return f;
+    };
+    for (int sb = s0; sb < s1; sb += 2 * kCH) {
+      __syncthreads();
+      if (threadIdx.x == 0) sh_n_irr = 0;
+      __syncthreads();
+      for (int i = threadIdx.x; i <= kCH; i += TB) {
+        double off[2][3];
+        bool valid[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int m = sb + i + h * kCH;
+          valid[h] = m < s1 && status[m].x != OV_EMPTY;
+          const d3 p = valid[h] ? ld3(pos, m) : O;
+          off[h][0] = p.x;
+          off[h][1] = p.y;
+          off[h][2] = p.z;
+        }
+        chain_node_set<true>(sh_node[i], off, valid);
+      }
+      for (int i = threadIdx.x; i < kCH; i += TB) {
+        float dd[2][3], f2v[2];
+        int idv[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int m = sb + i + h * kCH;
+          double d[3], far2 = 0;
+          const int f = seg_of(m, d, &far2);
+          dd[h][0] = dd[h][1] = dd[h][2] = 0.f;
+          f2v[h] = 0.f;
+          idv[h] = -1;
+          if (f < 0) continue;
+          if (f != m + 1) {
+            sh_irr_id[atomicAdd(&sh_n_irr, 1)] = m;
+            continue;
+          }
+          dd[h][0] = (float)d[0];
+          dd[h][1] = (float)d[1];
+          dd[h][2] = (float)d[2];
+          f2v[h] = (float)far2;
+          idv[h] = m;
+        }
+        chain_seg_set(sh_seg[i], dd, f2v, idv);
+      }
+      __syncthreads();
+      const int n_irr = sh_n_irr;
+      auto stage_slot = [&](int m) -> SrcVals {
+        double d[3], far2 = 0;
+        if (m < 0 || seg_of(m, d, &far2) < 0) return src_none();
+        const d3 a = ld3(pos, m);
+        return src_from(a.x, a.y, a.z, d[0], d[1], d[2], far2, m);
+      };
+      for (int q = threadIdx.x; 2 * q < n_irr; q += TB)
+        stage_pair(sh_irr[q], stage_slot(sh_irr_id[2 * q]),
+                   stage_slot(2 * q + 1 < n_irr ? sh_irr_id[2 * q + 1] : -1));
+      __syncthreads();
+      chain_sweep<true>(sh_node, sh_seg, T, acc, f4pi, special);
+      f2 b[kTT][3];
+#pragma unroll
+      for (int u = 0; u < kTT; ++u) b[u][0] = b[u][1] = b[u][2] = f2_splat(0.f);
+      for (int q = 0; 2 * q < n_irr; ++q) pair_interact<true>(sh_irr[q], T, b, special);
+#pragma unroll
+      for (int u = 0; u < kTT; ++u) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          float lo, hi;
+          f2_unpack(b[u][c], lo, hi);
+          acc[u][c] += f4pi * ((double)lo + (double)hi);
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) {
+      const int k = w.y + threadIdx.x + TB * u;
+      if (k < s1) st3(v_nl, k, kk[u] >= 0 ? mk3(acc[u][0], acc[u][1], acc[u][2]) : mk3(0, 0, 0));
+    }
+  }
+}
+
 // per system: near2 = (factor * longest segment)^2
 __global__ void k_sys_near2(const int* __restrict__ off, const double* __restrict__ pos,
                             const int2* __restrict__ links, const int2* __restrict__ status,
@@ -228,6 +371,11 @@ const Shape kShapes[] = {
     {256, 64, k_batch_bs64<256, 64>, k_batch_bs_mixed<256, 64>},
     {256, 128, k_batch_bs64<256, 128>, k_batch_bs_mixed<256, 128>},
     {256, 256, k_batch_bs64<256, 256>, k_batch_bs_mixed<256, 256>},
+    // sources_per_tile 0: the mixed form in chain order (tiles of 128
+    // segments); the FP64 form as with 128
+    {64, 0, k_batch_bs64<64, 128>, k_batch_bs_chain<64>},
+    {128, 0, k_batch_bs64<128, 128>, k_batch_bs_chain<128>},
+    {256, 0, k_batch_bs64<256, 128>, k_batch_bs_chain<256>},
 };
 constexpr int kNumShapes = sizeof(kShapes) / sizeof(kShapes[0]);
 

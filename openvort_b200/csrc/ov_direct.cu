@@ -222,50 +222,16 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_PAIRS_MIN_BLOCKS) k_direct_mixe
   }
 }
 
-// Mixed form in chain order (k_direct_mixed_chain).  Sources are staged in
-// slot order, where a loop's segments follow one another: segment m runs
-// from node m to node m + 1 for all but one segment per loop.  Such
-// "chained" segments share their end node with the next segment, so each
-// node's offset R = r_node - r, |R|^2 and 1/|R| are formed once per target
-// and used by both segments that touch it.  Per pair (a = |R|, b = |R'|):
-//   u = 1/(ab), den = 1 + R.R' u = 1 + cos, w = u / den
-//   v = kappa/4pi (1/a + 1/b) w (R x d)
-// R x d, with d the segment vector staged on its own, keeps the FP32 error
-// of the cross product at a few ulps of |R||d|.  1 - cos is first estimated
-// as 1 - R.R' u, whose error is below 1e-6; only a warp with a pair under
-// 2e-6 forms the exact |R x d|^2 u w of the reference's cut-off test.
-// That is 24 lane operations and 2 hardware approximations per interaction,
-// against 31 and 3 for the two-source form.  Segments that do not chain (a
-// loop's closing segment, a segment wrapped across a periodic face, a
-// tile's last segment) take the two-source form from a per-tile list.
-//
-// Tile layout: kCH chained pairs; pair i holds segments sb + i (low half)
-// and sb + kCH + i (high half), node pack i holds nodes sb + i and
-// sb + kCH + i, for i = 0 .. kCH.
-constexpr int kCH = kPSrc / 2;
-
-struct __align__(16) ChainSeg {
-  float4 a;      // dx0 dx1 dy0 dy1
-  float4 b;      // dz0 dz1 -dx0 -dx1
-  float4 c;      // -dy0 -dy1 -dz0 -dz1
-  float2 far2;   // FP32 far radius squared per half
-  int id[2];     // source slot, -1: contributes nothing
-};
-template <bool kTwo>
-struct __align__(8) ChainNode {
-  float2 x, y, z;            // offsets of the two nodes from the block origin
-  float2 lx[kTwo ? 1 : 0];   // two-float form: the low parts
-  float2 ly[kTwo ? 1 : 0];
-  float2 lz[kTwo ? 1 : 0];
-};
+// Mixed form in chain order (k_direct_mixed_chain, the sweep in
+// ov_pair.cuh): sources in slot order, each tile's chained segments swept
+// with shared end nodes and the others in the two-source form.  Targets as
+// in k_direct_mixed_pairs (key order, single-rounded offsets), or in slot
+// order with two-float offsets (no key sort needed).
+static_assert(2 * kCH == kPSrc, "a chain tile is the two-source form's tile");
 
 #ifndef OV_DIRECT_CHAIN_MIN_BLOCKS
 #define OV_DIRECT_CHAIN_MIN_BLOCKS 4
 #endif
-#ifndef OV_DIRECT_CHAIN_UNROLL
-#define OV_DIRECT_CHAIN_UNROLL 4
-#endif
-constexpr int kChainUnroll = OV_DIRECT_CHAIN_UNROLL;
 // kTwo: offsets as two floats (hi + lo) for targets and nodes, so R carries
 // ~2 ulps of |R| whatever the block's extent: targets may then come in slot
 // order (order == nullptr) with no key sort.
@@ -336,7 +302,6 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
     }
     return src_from(sg[0] - O.x, sg[1] - O.y, sg[2] - O.z, dxx, dyy, dzz, far2, id);
   };
-  const f2 one = f2_splat(1.0f), two = f2_splat(2.0f);
   for (int sb = s_lo; sb < s_hi; sb += kPSrc) {
     __syncthreads();
     if (threadIdx.x == 0) sh_n_irr = 0;
@@ -344,32 +309,18 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
     // node packs: nodes sb + i and sb + kCH + i (EMPTY or beyond the range:
     // far away, used by no chained segment)
     for (int i = threadIdx.x; i <= kCH; i += kPB) {
-      float o[2][3], lo[2][3];
+      double off[2][3];
+      bool valid[2];
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
         const int m = sb + i + h * kCH;
-        if (m < n_src && tstatus[m].x != OV_EMPTY) {
-          const d3 p = ld3(pos, m);
-          const double ox = p.x - O.x, oy = p.y - O.y, oz = p.z - O.z;
-          o[h][0] = (float)ox;
-          o[h][1] = (float)oy;
-          o[h][2] = (float)oz;
-          lo[h][0] = (float)(ox - o[h][0]);
-          lo[h][1] = (float)(oy - o[h][1]);
-          lo[h][2] = (float)(oz - o[h][2]);
-        } else {
-          o[h][0] = o[h][1] = o[h][2] = 1.0e4f;
-          lo[h][0] = lo[h][1] = lo[h][2] = 0.f;
-        }
+        valid[h] = m < n_src && tstatus[m].x != OV_EMPTY;
+        const d3 p = valid[h] ? ld3(pos, m) : O;
+        off[h][0] = p.x - O.x;
+        off[h][1] = p.y - O.y;
+        off[h][2] = p.z - O.z;
       }
-      sh_node[i].x = make_float2(o[0][0], o[1][0]);
-      sh_node[i].y = make_float2(o[0][1], o[1][1]);
-      sh_node[i].z = make_float2(o[0][2], o[1][2]);
-      if constexpr (kTwo) {
-        sh_node[i].lx[0] = make_float2(lo[0][0], lo[1][0]);
-        sh_node[i].ly[0] = make_float2(lo[0][1], lo[1][1]);
-        sh_node[i].lz[0] = make_float2(lo[0][2], lo[1][2]);
-      }
+      chain_node_set<kTwo>(sh_node[i], off, valid);
     }
     // chained segments; the others to the list
     for (int i = threadIdx.x; i < kCH; i += kPB) {
@@ -400,12 +351,7 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
         f2v[h] = (float)fmax(16.0 * (dxx * dxx + dyy * dyy + dzz * dzz), P.near2);
         idv[h] = m;
       }
-      sh_seg[i].a = make_float4(dd[0][0], dd[1][0], dd[0][1], dd[1][1]);
-      sh_seg[i].b = make_float4(dd[0][2], dd[1][2], -dd[0][0], -dd[1][0]);
-      sh_seg[i].c = make_float4(-dd[0][1], -dd[1][1], -dd[0][2], -dd[1][2]);
-      sh_seg[i].far2 = make_float2(f2v[0], f2v[1]);
-      sh_seg[i].id[0] = idv[0];
-      sh_seg[i].id[1] = idv[1];
+      chain_seg_set(sh_seg[i], dd, f2v, idv);
     }
     __syncthreads();
     const int n_irr = sh_n_irr;
@@ -413,108 +359,7 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
       stage_pair(sh_irr[q], stage_slot(sh_irr_id[2 * q]), 2 * q + 1 < n_irr ? stage_slot(sh_irr_id[2 * q + 1])
                                                                              : src_none());
     __syncthreads();
-    // node 0 of the tile for each target
-    f2 Rx[kTT], Ry[kTT], Rz[kTT], R2[kTT], ia[kTT];
-    {
-      const ChainNode<kTwo> nd = sh_node[0];
-      const f2 nx = f2_pack(nd.x.x, nd.x.y), ny = f2_pack(nd.y.x, nd.y.y), nz = f2_pack(nd.z.x, nd.z.y);
-#pragma unroll
-      for (int u = 0; u < kTT; ++u) {
-        Rx[u] = nx - T.x[u];
-        Ry[u] = ny - T.y[u];
-        Rz[u] = nz - T.z[u];
-        if constexpr (kTwo) {
-          Rx[u] = Rx[u] + (f2_pack(nd.lx[0].x, nd.lx[0].y) - T.lx[u]);
-          Ry[u] = Ry[u] + (f2_pack(nd.ly[0].x, nd.ly[0].y) - T.ly[u]);
-          Rz[u] = Rz[u] + (f2_pack(nd.lz[0].x, nd.lz[0].y) - T.lz[u]);
-        }
-        R2[u] = f2_fma(Rz[u], Rz[u], f2_fma(Ry[u], Ry[u], Rx[u] * Rx[u]));
-        ia[u] = f2_rsqrt(R2[u]);
-      }
-    }
-    // FP32 partial sums over 32 segments, each added into the FP64 sums
-    for (int i0 = 0; i0 < kCH; i0 += 16) {
-      f2 b[kTT][3];
-#pragma unroll
-      for (int u = 0; u < kTT; ++u) b[u][0] = b[u][1] = b[u][2] = f2_splat(0.f);
-#pragma unroll kChainUnroll
-      for (int i = i0; i < i0 + 16; ++i) {
-        const ChainNode<kTwo> nd = sh_node[i + 1];
-        const ChainSeg sg = sh_seg[i];
-        const f2 nx = f2_pack(nd.x.x, nd.x.y), ny = f2_pack(nd.y.x, nd.y.y), nz = f2_pack(nd.z.x, nd.z.y);
-        f2 nlx, nly, nlz;
-        if constexpr (kTwo) {
-          nlx = f2_pack(nd.lx[0].x, nd.lx[0].y);
-          nly = f2_pack(nd.ly[0].x, nd.ly[0].y);
-          nlz = f2_pack(nd.lz[0].x, nd.lz[0].y);
-        }
-        const f2 dx = f2_pack(sg.a.x, sg.a.y), dy = f2_pack(sg.a.z, sg.a.w), dz = f2_pack(sg.b.x, sg.b.y);
-        const f2 ndx = f2_pack(sg.b.z, sg.b.w), ndy = f2_pack(sg.c.x, sg.c.y), ndz = f2_pack(sg.c.z, sg.c.w);
-#pragma unroll
-        for (int u = 0; u < kTT; ++u) {
-          f2 Bx = nx - T.x[u], By = ny - T.y[u], Bz = nz - T.z[u];
-          if constexpr (kTwo) {
-            Bx = Bx + (nlx - T.lx[u]);
-            By = By + (nly - T.ly[u]);
-            Bz = Bz + (nlz - T.lz[u]);
-          }
-          const f2 B2 = f2_fma(Bz, Bz, f2_fma(By, By, Bx * Bx));
-          const f2 ib = f2_rsqrt(B2);
-          const f2 Cx = f2_fma(Ry[u], dz, Rz[u] * ndy);
-          const f2 Cy = f2_fma(Rz[u], dx, Rx[u] * ndz);
-          const f2 Cz = f2_fma(Rx[u], dy, Ry[u] * ndx);
-          const f2 e = f2_fma(Rz[u], Bz, f2_fma(Ry[u], By, Rx[u] * Bx));
-          const f2 uu = ia[u] * ib;
-          const f2 den = f2_fma(e, uu, one);
-          const f2 w = uu * f2_rcp(den);
-          const f2 s = (ia[u] + ib) * w;
-          const f2 est = two - den;   // 1 - cos, error below 1e-6
-          float r20, r21, s0, s1, e0, e1;
-          f2_unpack(R2[u], r20, r21);
-          f2_unpack(s, s0, s1);
-          f2_unpack(est, e0, e1);
-          bool far0 = r20 >= sg.far2.x && sg.id[0] >= 0, far1 = r21 >= sg.far2.y && sg.id[1] >= 0;
-          bool ok0 = far0 && e0 > 2e-6f, ok1 = far1 && e1 > 2e-6f;
-          bool sp0 = sg.id[0] >= 0 && !far0, sp1 = sg.id[1] >= 0 && !far1;
-          if (__any_sync(0xffffffffu, (far0 && !ok0) || (far1 && !ok1))) {
-            // near the colinearity cut-off: the exact 1 - cos = |C|^2 u w
-            const f2 tc = f2_fma(Cz, Cz, f2_fma(Cy, Cy, Cx * Cx)) * (uu * w);
-            float tc0, tc1;
-            f2_unpack(tc, tc0, tc1);
-            if (far0 && !ok0) {
-              ok0 = tc0 > kColHi;
-              sp0 = !ok0 && !(tc0 < kColLo);
-            }
-            if (far1 && !ok1) {
-              ok1 = tc1 > kColHi;
-              sp1 = !ok1 && !(tc1 < kColLo);
-            }
-          }
-          const f2 sk = f2_pack(ok0 ? s0 : 0.f, ok1 ? s1 : 0.f);
-          b[u][0] = f2_fma(Cx, sk, b[u][0]);
-          b[u][1] = f2_fma(Cy, sk, b[u][1]);
-          b[u][2] = f2_fma(Cz, sk, b[u][2]);
-          if (sp0 || sp1) {
-            if (sp0) special(u, sg.id[0]);
-            if (sp1) special(u, sg.id[1]);
-          }
-          Rx[u] = Bx;
-          Ry[u] = By;
-          Rz[u] = Bz;
-          R2[u] = B2;
-          ia[u] = ib;
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < kTT; ++u) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          float lo, hi;
-          f2_unpack(b[u][c], lo, hi);
-          acc[u][c] += f4pi * ((double)lo + (double)hi);
-        }
-      }
-    }
+    chain_sweep<kTwo>(sh_node, sh_seg, T, acc, f4pi, special);
     // the segments that do not chain, two per record
     {
       f2 b[kTT][3];

@@ -210,3 +210,194 @@ __device__ __forceinline__ void pair_interact(const PairSrc<kTwo>& src, const Pa
     }
   }
 }
+
+// ----------------------------------------------------------------------
+// Chain order: sources staged in slot order, where a loop's segments
+// follow one another, so segment m runs from node m to node m + 1 for all
+// but one segment per loop ("chained").  Each node's offset R = r_node - r,
+// |R|^2 and 1/|R| are formed once per target and serve both segments that
+// touch it.  Per pair (a = |R|, b = |R'|):
+//   u = 1/(ab), den = 1 + R.R' u = 1 + cos, w = u / den
+//   v = kappa/4pi (1/a + 1/b) w (R x d)
+// R x d, with the segment vector d staged on its own, keeps the FP32 error
+// of the cross product at a few ulps of |R||d|.  1 - cos is first estimated
+// as 2 - den, whose error is below 1e-6; only a warp with a pair under
+// 2e-6 forms the exact |R x d|^2 u w of the reference's cut-off test
+// (src/tangle.c:505-506).  That is 24 lane operations and 2 hardware
+// approximations per interaction, against 31 and 3 for the two-source form
+// above.  Segments that do not chain (a loop's closing segment, a segment
+// wrapped across a periodic face) take the two-source form from a list.
+//
+// A tile holds kCH chained pairs: pair i is segments sb + i (low half) and
+// sb + kCH + i (high half); node pack i is nodes sb + i and sb + kCH + i,
+// i = 0 .. kCH.
+constexpr int kCH = 64;
+
+#ifndef OV_CHAIN_UNROLL
+#define OV_CHAIN_UNROLL 4
+#endif
+constexpr int kChainUnroll = OV_CHAIN_UNROLL;
+
+struct __align__(16) ChainSeg {
+  float4 a;      // dx0 dx1 dy0 dy1
+  float4 b;      // dz0 dz1 -dx0 -dx1
+  float4 c;      // -dy0 -dy1 -dz0 -dz1
+  float2 far2;   // FP32 far radius squared per half
+  int id[2];     // source slot, -1: contributes nothing
+};
+template <bool kTwo>
+struct __align__(8) ChainNode {
+  float2 x, y, z;            // offsets of the two nodes from the block origin
+  float2 lx[kTwo ? 1 : 0];   // two-float form: the low parts
+  float2 ly[kTwo ? 1 : 0];
+  float2 lz[kTwo ? 1 : 0];
+};
+
+
+// node pack: two node offsets from the origin (hi, and lo parts in the
+// two-float form); `valid` false places the node far away, used by no
+// chained segment
+template <bool kTwo>
+__device__ __forceinline__ void chain_node_set(ChainNode<kTwo>& nd, const double (&off)[2][3],
+                                               const bool (&valid)[2]) {
+  float o[2][3], lo[2][3];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      o[h][c] = valid[h] ? (float)off[h][c] : 1.0e4f;
+      lo[h][c] = valid[h] ? (float)(off[h][c] - (double)o[h][c]) : 0.f;
+    }
+  nd.x = make_float2(o[0][0], o[1][0]);
+  nd.y = make_float2(o[0][1], o[1][1]);
+  nd.z = make_float2(o[0][2], o[1][2]);
+  if constexpr (kTwo) {
+    nd.lx[0] = make_float2(lo[0][0], lo[1][0]);
+    nd.ly[0] = make_float2(lo[0][1], lo[1][1]);
+    nd.lz[0] = make_float2(lo[0][2], lo[1][2]);
+  }
+}
+
+// chained pair: segment vectors, FP32 far radii and slots (-1: none)
+__device__ __forceinline__ void chain_seg_set(ChainSeg& sg, const float (&dd)[2][3], const float (&far2)[2],
+                                              const int (&id)[2]) {
+  sg.a = make_float4(dd[0][0], dd[1][0], dd[0][1], dd[1][1]);
+  sg.b = make_float4(dd[0][2], dd[1][2], -dd[0][0], -dd[1][0]);
+  sg.c = make_float4(-dd[0][1], -dd[1][1], -dd[0][2], -dd[1][2]);
+  sg.far2 = make_float2(far2[0], far2[1]);
+  sg.id[0] = id[0];
+  sg.id[1] = id[1];
+}
+
+// The kCH chained pairs of a staged tile against the thread's targets:
+// FP32 partial sums over 32 segments, each added (times f4pi) into acc;
+// pairs needing FP64 call special(u, slot).  Every thread of the warp runs
+// the same iterations.
+template <bool kTwo, class Special>
+__device__ __forceinline__ void chain_sweep(const ChainNode<kTwo>* sh_node, const ChainSeg* sh_seg,
+                                            const PairTargets& T, double (&acc)[kTT][3], double f4pi,
+                                            Special&& special) {
+  const f2 one = f2_splat(1.0f), two = f2_splat(2.0f);
+  // node 0 of the tile for each target
+  f2 Rx[kTT], Ry[kTT], Rz[kTT], R2[kTT], ia[kTT];
+  {
+    const ChainNode<kTwo> nd = sh_node[0];
+    const f2 nx = f2_pack(nd.x.x, nd.x.y), ny = f2_pack(nd.y.x, nd.y.y), nz = f2_pack(nd.z.x, nd.z.y);
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) {
+      Rx[u] = nx - T.x[u];
+      Ry[u] = ny - T.y[u];
+      Rz[u] = nz - T.z[u];
+      if constexpr (kTwo) {
+        Rx[u] = Rx[u] + (f2_pack(nd.lx[0].x, nd.lx[0].y) - T.lx[u]);
+        Ry[u] = Ry[u] + (f2_pack(nd.ly[0].x, nd.ly[0].y) - T.ly[u]);
+        Rz[u] = Rz[u] + (f2_pack(nd.lz[0].x, nd.lz[0].y) - T.lz[u]);
+      }
+      R2[u] = f2_fma(Rz[u], Rz[u], f2_fma(Ry[u], Ry[u], Rx[u] * Rx[u]));
+      ia[u] = f2_rsqrt(R2[u]);
+    }
+  }
+  // FP32 partial sums over 32 segments, each added into the FP64 sums
+  for (int i0 = 0; i0 < kCH; i0 += 16) {
+    f2 b[kTT][3];
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) b[u][0] = b[u][1] = b[u][2] = f2_splat(0.f);
+#pragma unroll kChainUnroll
+    for (int i = i0; i < i0 + 16; ++i) {
+      const ChainNode<kTwo> nd = sh_node[i + 1];
+      const ChainSeg sg = sh_seg[i];
+      const f2 nx = f2_pack(nd.x.x, nd.x.y), ny = f2_pack(nd.y.x, nd.y.y), nz = f2_pack(nd.z.x, nd.z.y);
+      f2 nlx, nly, nlz;
+      if constexpr (kTwo) {
+        nlx = f2_pack(nd.lx[0].x, nd.lx[0].y);
+        nly = f2_pack(nd.ly[0].x, nd.ly[0].y);
+        nlz = f2_pack(nd.lz[0].x, nd.lz[0].y);
+      }
+      const f2 dx = f2_pack(sg.a.x, sg.a.y), dy = f2_pack(sg.a.z, sg.a.w), dz = f2_pack(sg.b.x, sg.b.y);
+      const f2 ndx = f2_pack(sg.b.z, sg.b.w), ndy = f2_pack(sg.c.x, sg.c.y), ndz = f2_pack(sg.c.z, sg.c.w);
+#pragma unroll
+      for (int u = 0; u < kTT; ++u) {
+        f2 Bx = nx - T.x[u], By = ny - T.y[u], Bz = nz - T.z[u];
+        if constexpr (kTwo) {
+          Bx = Bx + (nlx - T.lx[u]);
+          By = By + (nly - T.ly[u]);
+          Bz = Bz + (nlz - T.lz[u]);
+        }
+        const f2 B2 = f2_fma(Bz, Bz, f2_fma(By, By, Bx * Bx));
+        const f2 ib = f2_rsqrt(B2);
+        const f2 Cx = f2_fma(Ry[u], dz, Rz[u] * ndy);
+        const f2 Cy = f2_fma(Rz[u], dx, Rx[u] * ndz);
+        const f2 Cz = f2_fma(Rx[u], dy, Ry[u] * ndx);
+        const f2 e = f2_fma(Rz[u], Bz, f2_fma(Ry[u], By, Rx[u] * Bx));
+        const f2 uu = ia[u] * ib;
+        const f2 den = f2_fma(e, uu, one);
+        const f2 w = uu * f2_rcp(den);
+        const f2 s = (ia[u] + ib) * w;
+        const f2 est = two - den;   // 1 - cos, error below 1e-6
+        float r20, r21, s0, s1, e0, e1;
+        f2_unpack(R2[u], r20, r21);
+        f2_unpack(s, s0, s1);
+        f2_unpack(est, e0, e1);
+        bool far0 = r20 >= sg.far2.x && sg.id[0] >= 0, far1 = r21 >= sg.far2.y && sg.id[1] >= 0;
+        bool ok0 = far0 && e0 > 2e-6f, ok1 = far1 && e1 > 2e-6f;
+        bool sp0 = sg.id[0] >= 0 && !far0, sp1 = sg.id[1] >= 0 && !far1;
+        if (__any_sync(0xffffffffu, (far0 && !ok0) || (far1 && !ok1))) {
+          // near the colinearity cut-off: the exact 1 - cos = |C|^2 u w
+          const f2 tc = f2_fma(Cz, Cz, f2_fma(Cy, Cy, Cx * Cx)) * (uu * w);
+          float tc0, tc1;
+          f2_unpack(tc, tc0, tc1);
+          if (far0 && !ok0) {
+            ok0 = tc0 > kColHi;
+            sp0 = !ok0 && !(tc0 < kColLo);
+          }
+          if (far1 && !ok1) {
+            ok1 = tc1 > kColHi;
+            sp1 = !ok1 && !(tc1 < kColLo);
+          }
+        }
+        const f2 sk = f2_pack(ok0 ? s0 : 0.f, ok1 ? s1 : 0.f);
+        b[u][0] = f2_fma(Cx, sk, b[u][0]);
+        b[u][1] = f2_fma(Cy, sk, b[u][1]);
+        b[u][2] = f2_fma(Cz, sk, b[u][2]);
+        if (sp0 || sp1) {
+          if (sp0) special(u, sg.id[0]);
+          if (sp1) special(u, sg.id[1]);
+        }
+        Rx[u] = Bx;
+        Ry[u] = By;
+        Rz[u] = Bz;
+        R2[u] = B2;
+        ia[u] = ib;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kTT; ++u) {
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        float lo, hi;
+        f2_unpack(b[u][c], lo, hi);
+        acc[u][c] += f4pi * ((double)lo + (double)hi);
+      }
+    }
+  }
+}

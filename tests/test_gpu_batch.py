@@ -141,7 +141,7 @@ def test_batch_autotune_keeps_results(ov, ensemble):
     b.download()
     v0 = b.t.vels.copy()
     tu = b.autotune()
-    assert tu.targets_per_block in (64, 128, 256) and tu.sources_per_tile in (64, 128, 256)
+    assert tu.targets_per_block in (64, 128, 256) and tu.sources_per_tile in (0, 64, 128, 256)
     assert tu.kernel_ms > 0
     b.update(0.0)
     b.download()
@@ -153,12 +153,33 @@ def test_batch_autotune_keeps_results(ov, ensemble):
     b.update(0.0)
     b.download()
     v64 = b.t.vels.copy()
-    for shape in ((64, 64), (256, 256), (128, 64)):
+    for shape in ((64, 64), (256, 256), (128, 64), (128, 0)):
         b.set_tuning(*shape)
         b.update(0.0)
         b.download()
         assert np.array_equal(b.t.vels, v64)
     b.close()
+
+
+@pytest.mark.parametrize("tb", [64, 128, 256])
+def test_batch_chain_order_mixed_vs_fp64(ov, ensemble, tb):
+    """The chain-order mixed kernel (sources_per_tile 0) within the mixed
+    tolerance of the FP64 sums."""
+    t, off, _ = ensemble
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
+    b = ov.DeviceBatch(t.copy(), off)
+    b.update(0.0)
+    b.download()
+    v64 = b.t.vels.copy()
+    b.close()
+    ov.configure(PARAMS, ov.OV_PREC_MIXED)
+    b = ov.DeviceBatch(t.copy(), off)
+    b.set_tuning(tb, 0)
+    b.update(0.0)
+    b.download()
+    assert rel_err(b.t.vels, v64) < TOL_MIXED
+    b.close()
+    ov.configure(PARAMS, ov.OV_PREC_FP64)
 
 
 def test_batch_rejects_bad_ensembles(ov, ensemble, monkeypatch):
