@@ -4,30 +4,11 @@
 // All FP64; each thread owns one node slot.  HBM-bound: ~150 B per node.
 #include "ov_internal.h"
 #include "ov_links.cuh"
+#include "ov_node.cuh"
 
 namespace {
 
 constexpr int kThreads = 256;
-
-// s' and s'' at x=0 from four points p_j at arc offsets x_j: weights are the
-// first and second derivatives at 0 of the Lagrange basis through {0, x_j}
-// (the 4-point non-uniform stencils of src/tangle.c:312-344,434-470).
-__device__ void stencil4(const OvParams& P, d3 s0, const d3 p[4], const double x[4],
-                         d3& tan, d3& nrm) {
-  d3 a = mk3(0, 0, 0), b = mk3(0, 0, 0);
-#pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    double o0 = x[(j + 1) & 3], o1 = x[(j + 2) & 3], o2 = x[(j + 3) & 3];
-    double den = x[j] * (x[j] - o0) * (x[j] - o1) * (x[j] - o2);
-    double w1 = -(o0 * o1 * o2) / den;
-    double w2 = 2.0 * (o0 * o1 + o0 * o2 + o1 * o2) / den;
-    d3 d = pwrap(P, p[j], s0) - p[j];   // s0 - p_j (wrapped)
-    a = a + d * (-w1);
-    b = b + d * (-w2);
-  }
-  tan = a;
-  nrm = b;
-}
 
 // idx: the slots to compute (null: slots 0 .. n-1)
 __global__ void k_dxi(OvParams P, Links L, const double* __restrict__ pos, double* dxi,
@@ -36,10 +17,9 @@ __global__ void k_dxi(OvParams P, Links L, const double* __restrict__ pos, doubl
   if (i >= n) return;
   const int k = idx ? idx[i] : i;
   if (L.st[k].x == OV_EMPTY) return;
-  d3 s0 = ld3(pos, k), s1;
-  if (!step_node(P, L, pos, k, 1, s1)) { atomicOr(flag, 1); return; }
-  d3 w = pwrap(P, s0, s1);
-  dxi[k] = norm_ref(s0 - w);
+  double d;
+  if (!dxi_node(P, L, pos, k, d)) { atomicOr(flag, 1); return; }
+  dxi[k] = d;
 }
 
 // pass 0: pinned and ordinary nodes; pass 1: nodes next to a pinned node,
@@ -52,56 +32,10 @@ __global__ void k_tangents(OvParams P, Links L, const double* __restrict__ pos,
   const int k = idx ? idx[i] : i;
   int2 st = L.st[k];
   if (st.x == OV_EMPTY) return;
-  int2 lk = L.lk[k];
-  bool near_pin = st.x != OV_PINNED &&
-                  ((lk.x >= 0 && L.st[lk.x].x == OV_PINNED) || (lk.y >= 0 && L.st[lk.y].x == OV_PINNED));
-  if ((pass == 1) != near_pin) return;
-  d3 s0 = ld3(pos, k), t, nn;
-  bool ok = true;
-  if (st.x == OV_PINNED) {
-    // one-sided stencil away from the wall (src/tangle.c:275-364); the
-    // reference tests forward > 0, so a forward link to slot 0 goes backwards
-    int dir = lk.x > 0 ? 1 : -1;
-    d3 p[4];
-    double x[4];
-    for (int j = 0; j < 4 && ok; ++j) {
-      double a;
-      ok = ok && arc_length(L, dxi, k, dir * (j + 1), a) && step_node(P, L, pos, k, dir * (j + 1), p[j]);
-      x[j] = dir * a;
-    }
-    if (ok) stencil4(P, s0, p, x, t, nn);
-  } else if (near_pin) {
-    d3 s1, sm1;
-    double a, bm;
-    ok = step_node(P, L, pos, k, 1, s1) && step_node(P, L, pos, k, -1, sm1) &&
-         arc_length(L, dxi, k, 1, a) && arc_length(L, dxi, k, -1, bm);
-    if (ok) {
-      double b = -bm;
-      d3 ds1 = pwrap(P, s1, s0) - s1, dsm1 = pwrap(P, sm1, s0) - sm1;
-      d3 t1 = ld3(tan, lk.x), tm1 = ld3(tan, lk.y);
-      double h = a - b, h2 = h * h, h3 = h2 * h;
-      double ct1 = -b * b / h2, ctm1 = -a * a / h2;
-      double cs1 = 2 * b * b * (b - 2 * a) / (a * h3);
-      double csm1 = 2 * a * a * (2 * b - a) / (b * h3);
-      double cn1 = 2 * b * (8 * a * a - a * b - b * b) / (a * a * h3);
-      double cnm1 = 2 * a * (a * a + a * b - 8 * b * b) / (b * b * h3);
-      double cnt1 = 2 * b * (2 * a + b) / (a * h2);
-      double cntm1 = 2 * a * (a + 2 * b) / (b * h2);
-      t = (t1 * ct1 + tm1 * ctm1) + (ds1 * cs1 + dsm1 * csm1);
-      nn = (t1 * cnt1 + tm1 * cntm1) + (ds1 * cn1 + dsm1 * cnm1);
-    }
-  } else {
-    const int off[4] = {2, 1, -1, -2};
-    d3 p[4];
-    double x[4];
-    for (int j = 0; j < 4 && ok; ++j) {
-      double a;
-      ok = ok && arc_length(L, dxi, k, off[j], a) && step_node(P, L, pos, k, off[j], p[j]);
-      x[j] = off[j] > 0 ? a : -a;
-    }
-    if (ok) stencil4(P, s0, p, x, t, nn);
-  }
-  if (!ok) { atomicOr(flag, 1); return; }
+  if ((pass == 1) != near_pinned(L, k)) return;
+  d3 t, nn;
+  auto arc = [&](int kk, int dist, double& out) { return arc_length(L, dxi, kk, dist, out); };
+  if (!tangent_node(P, L, pos, k, arc, tan, t, nn)) { atomicOr(flag, 1); return; }
   st3(tan, k, t);
   st3(nrm, k, nn);
 }
@@ -117,44 +51,13 @@ __global__ void k_epilogue(OvParams P, Links L, const double* __restrict__ t_dev
   if (i >= k1) return;
   const int k = idx ? idx[i] : i;
   const double t = t_dev ? t0 + *t_dev : t0;
-  int2 st = L.st[k];
-  if (st.x == OV_EMPTY) return;
-  d3 r = ld3(pos, k);
-  if (st.x == OV_PINNED) {
-    st3(vs_out, k, mk3(0, 0, 0));
-    st3(vels, k, flow_eval(P.vb, r, t));
-    return;
-  }
-  d3 tg = ld3(tan, k), nm = ld3(nrm, k);
-  // local induction (lia_velocity, src/tangle.c:530-551)
-  d3 nx, pv;
-  if (!step_node(P, L, pos, k, 1, nx) || !step_node(P, L, pos, k, -1, pv)) {
-    atomicOr(flag, 1);
-    return;
-  }
-  double l_next = norm_ref(r - pwrap(P, r, nx));
-  double l_prev = norm_ref(pv - pwrap(P, pv, r));
-  double f = P.kappa * log(2.0 * sqrt(l_next * l_prev) / sqrt(sqrt(OV_E)) / P.core_a) / 4.0 / OV_PI;
-  d3 lia = cross3(tg, nm) * f;
-  d3 vs = lia + flow_eval(P.vs, r, t);
-  if (!P.lia_only) {
-    vs = vs + ld3(v_nl, k);
-    if (P.n_img > 0) vs = vs + ld3(v_img, k);
-  }
-  d3 v = vs;
-  if (P.hyperfriction) {
-    if (norm_ref(nm) > P.max_curv / P.dl_max) v = v + cross3(tg, lia) * (-P.hyperalpha);
-  }
-  if (P.use_mf) {
-    d3 dv = flow_eval(P.vn, r, t) - vs;
-    v = v + cross3(tg, dv) * P.alpha;
-    v = v + cross3(tg, cross3(tg, dv)) * (-P.alpha_p);
-  }
-  if (st.x == OV_PINNED_SLIP) {
-    d3 nw = face_normal(st.y);
-    v = v - nw * dot3(nw, v);
-  }
-  if (!(isfinite(v.x) && isfinite(v.y) && isfinite(v.z))) atomicOr(flag, 2);
+  if (L.st[k].x == OV_EMPTY) return;
+  const d3 vnl = P.lia_only ? mk3(0, 0, 0) : ld3(v_nl, k);
+  const d3 vim = (P.lia_only || P.n_img == 0) ? mk3(0, 0, 0) : ld3(v_img, k);
+  d3 v, vs;
+  const int err = epilogue_node(P, L, t, pos, k, ld3(tan, k), ld3(nrm, k), vnl, vim, v, vs);
+  if (err & 1) { atomicOr(flag, 1); return; }
+  if (err) atomicOr(flag, err);
   st3(vs_out, k, vs);
   st3(vels, k, v);
 }

@@ -147,20 +147,32 @@ __global__ void k_rec_scan(OvParams P, Grid g, const double* __restrict__ pos, c
 // (local term, flows, friction) then follows on the current links.
 
 // targets of a batch: node positions, each skipping its own segments
-__global__ void k_rec_points(const int* __restrict__ nodes, int count, const double* __restrict__ pos,
-                             double* pts, int* skip) {
+// Every kernel below checks each listed slot against n (flag bit 1 and no
+// access when outside), so a wrong list is an error, not a stray access.
+__global__ void k_rec_points(const int* __restrict__ nodes, int count, int n, const double* __restrict__ pos,
+                             double* pts, int* skip, int* flag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int k = nodes[i];
+  if (k < 0 || k >= n) {
+    atomicOr(flag, 1);
+    pts[3 * i] = pts[3 * i + 1] = pts[3 * i + 2] = 0;
+    skip[i] = -1;
+    return;
+  }
   st3(pts, i, ld3(pos, k));
   skip[i] = k;
 }
 
-__global__ void k_rec_scatter(const int* __restrict__ nodes, int count, const double* __restrict__ nl,
-                              const double* __restrict__ img, double* v_nl, double* v_img) {
+__global__ void k_rec_scatter(const int* __restrict__ nodes, int count, int n, const double* __restrict__ nl,
+                              const double* __restrict__ img, double* v_nl, double* v_img, int* flag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int k = nodes[i];
+  if (k < 0 || k >= n) {
+    atomicOr(flag, 1);
+    return;
+  }
   st3(v_nl, k, ld3(nl, i));
   st3(v_img, k, ld3(img, i));
 }
@@ -175,11 +187,17 @@ struct SegChange {
 // v_nl and v_img of the listed nodes += the changed segments' fields, with
 // the skip rule of the tangle's own sum (src/tangle.c:614-616) and the
 // mirror reflection of each image's sum (src/tangle.c:633-634)
-__global__ void k_rec_correct(OvParams P, SegChange C, const int* __restrict__ nodes, int count,
-                              const double* __restrict__ pos, double* v_nl, double* v_img) {
+__global__ void k_rec_correct(OvParams P, SegChange C, const int* __restrict__ nodes, int count, int n,
+                              const double* __restrict__ pos, double* v_nl, double* v_img, int* flag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int k = nodes[i];
+  bool ok = k >= 0 && k < n;
+  for (int c = 0; c < 4; ++c) ok = ok && C.m[c] >= 0 && C.m[c] < n && C.f[c] >= 0 && C.f[c] < n;
+  if (!ok) {
+    atomicOr(flag, 1);
+    return;
+  }
   const d3 r = ld3(pos, k);
   d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
   for (int c = 0; c < 4; ++c) {
@@ -198,11 +216,16 @@ __global__ void k_rec_correct(OvParams P, SegChange C, const int* __restrict__ n
 }
 
 // vels and vs of the listed nodes, packed 6 doubles per node for one copy
-__global__ void k_rec_pack(const int* __restrict__ nodes, int count, const double* __restrict__ vels,
-                           const double* __restrict__ vs, double* out) {
+__global__ void k_rec_pack(const int* __restrict__ nodes, int count, int n, const double* __restrict__ vels,
+                           const double* __restrict__ vs, double* out, int* flag) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const int k = nodes[i];
+  if (k < 0 || k >= n) {
+    atomicOr(flag, 1);
+    for (int c = 0; c < 6; ++c) out[6 * (size_t)i + c] = 0;
+    return;
+  }
   st3(out + 6 * (size_t)i, 0, ld3(vels, k));
   st3(out + 6 * (size_t)i + 3, 0, ld3(vs, k));
 }
@@ -363,16 +386,16 @@ bool refresh_known(RecState& R, RecVel& V) {
   ov_state_impl* s = &R.s;
   const int cnt = (int)V.known.size();
   if (cnt == 0) return true;
+  // the pass's error flag (zeroed at its start) accumulates every kernel's bits
   int* flag = s->dflag.as<int>();
-  OV_TRY_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), s->stream));
   if (!ov_launch_epilogue_list(s->stream, s->P, s->links.as<int2>(), s->status.as<int2>(), V.time,
                                s->pos.as<double>(), s->tan.as<double>(), s->nrm.as<double>(),
                                s->v_nl.as<double>(), s->v_img.as<double>(), s->vels.as<double>(),
                                s->vs.as<double>(), R.known.as<int>(), cnt, flag))
     return false;
   if (!R.pack.reserve(sizeof(double) * 6 * (size_t)cnt + 64)) return false;
-  k_rec_pack<<<(cnt + 255) / 256, 256, 0, s->stream>>>(R.known.as<int>(), cnt, s->vels.as<double>(),
-                                                       s->vs.as<double>(), R.pack.as<double>());
+  k_rec_pack<<<(cnt + 255) / 256, 256, 0, s->stream>>>(R.known.as<int>(), cnt, s->n, s->vels.as<double>(),
+                                                       s->vs.as<double>(), R.pack.as<double>(), flag);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   int h_flag = 0;
@@ -401,18 +424,20 @@ bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes) {
       !R.skip.reserve(sizeof(int) * (size_t)m) || !R.bnl.reserve(sizeof(double) * 3 * (size_t)m) ||
       !R.bimg.reserve(sizeof(double) * 3 * (size_t)m))
     return false;
-  OV_TRY_CUDA(cudaMemcpyAsync(R.known.as<int>() + old, V.known.data() + old, sizeof(int) * (size_t)m,
+  // the whole list: growing R.known reallocates it without its contents
+  OV_TRY_CUDA(cudaMemcpyAsync(R.known.as<int>(), V.known.data(), sizeof(int) * (size_t)cnt,
                               cudaMemcpyHostToDevice, s->stream));
   const int* batch = R.known.as<int>() + old;
   if (!s->P.lia_only) {
-    k_rec_points<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->pos.as<double>(), R.pts.as<double>(),
-                                                          R.skip.as<int>());
+    k_rec_points<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->n, s->pos.as<double>(),
+                                                          R.pts.as<double>(), R.skip.as<int>(), s->dflag.as<int>());
     OV_LAUNCHED();
     if (!ov_direct_points(s, s->pos.as<double>(), m, R.pts.as<double>(), R.skip.as<int>(), nullptr, 0,
                           R.bnl.as<double>(), R.bimg.as<double>()))
       return false;
-    k_rec_scatter<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, R.bnl.as<double>(), R.bimg.as<double>(),
-                                                           s->v_nl.as<double>(), s->v_img.as<double>());
+    k_rec_scatter<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->n, R.bnl.as<double>(),
+                                                           R.bimg.as<double>(), s->v_nl.as<double>(),
+                                                           s->v_img.as<double>(), s->dflag.as<int>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
   }
@@ -452,6 +477,8 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
   if (!upload_for_pass(R, tangle) || !find_candidates(R, tangle, rec_dist, rec_angle, cand))
     return -ov_last_error();
   ov_state_impl* s = &R.s;
+  if (!ov_cuda_ok(cudaMemsetAsync(s->dflag.p, 0, sizeof(int), s->stream), "cudaMemsetAsync"))
+    return -ov_last_error();
   RecVel V;
   V.pos_of.assign(tangle->N, -1);
   V.time = t;
@@ -533,8 +560,9 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     C.m[3] = changed[3]; C.f[3] = tangle->connections[changed[3]].forward; C.sign[3] = 1;
     const int cnt = (int)V.known.size();
     if (cnt > 0 && !s->P.lia_only) {
-      k_rec_correct<<<(cnt + 127) / 128, 128, 0, s->stream>>>(s->P, C, R.known.as<int>(), cnt, s->pos.as<double>(),
-                                                               s->v_nl.as<double>(), s->v_img.as<double>());
+      k_rec_correct<<<(cnt + 127) / 128, 128, 0, s->stream>>>(s->P, C, R.known.as<int>(), cnt, s->n,
+                                                               s->pos.as<double>(), s->v_nl.as<double>(),
+                                                               s->v_img.as<double>(), s->dflag.as<int>());
       OV_LAUNCHED();
       if (!ov_cuda_ok(cudaGetLastError(), "k_rec_correct")) return -ov_last_error();
     }

@@ -20,7 +20,6 @@
 // segments in FP32 from FP64-formed relative vectors, FP64 sums; the opening
 // test and near segments (|R| < 4 |ds|) in FP64.
 #include <float.h>
-#include <stdlib.h>
 
 #include <algorithm>
 
@@ -447,11 +446,14 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
               const float fnear2 = (float)near2;
               // two (x, y) columns per packed FP32 pair: columns 2g and 2g + 1
               // (the last group has column 8 only), their three z images
-              // evaluated side by side (independent chains), each image's
-              // terms summed where it accepts the cell
-              const f2 g0s = f2_splat(g0), g1s = f2_splat(g1), g2s = f2_splat(g2);
-              const f2 m02s = f2_splat(m02), m12s = f2_splat(m12), m22s = f2_splat(m22), m21s = f2_splat(m21);
-              f2 accx = f2_splat(0.f), accy = f2_splat(0.f), accz = f2_splat(0.f);
+              // evaluated side by side (independent chains).  The 27 image
+              // terms are summed in factored form: with i3 = |R|^-3 and
+              // i5 = R_z |R|^-5 per image, the reference's
+              // ((g + m R_z/|R|^2) x R + (m21, 0, 0)) i3 summed over the images
+              // is g x P + m x Q + (m21 S, 0, 0), P = sum i3 R, Q = sum i5 R,
+              // S = sum i3; since R_x and R_y are constant along a column,
+              // P_x, P_y, Q_x, Q_y take each column's sums of i3 and i5 once.
+              f2 px = f2_splat(0.f), py = px, pz = px, qx = px, qy = px, qz = px, sv = px;
               // All 27 images accept (the usual case: the wrapped opening test
               // treats every image point like the target) and none is near:
               // no per-image masks or near-field tests.  An image shifted
@@ -476,25 +478,28 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
                   const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
                   const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
                   const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
-                  const f2 nX = f2_pack(-Xa, -Xb), nY = f2_pack(-Ya, -Yb);
                   const f2 XY2 = f2_fma(X, X, Y * Y);
                   // the last group holds column 8 twice: its second half is dropped
                   const f2 keep = f2_pack(1.f, grp < 4 ? 1.f : 0.f);
+                  f2 c3 = f2_splat(0.f), c5 = c3;
 #pragma unroll
                   for (int iz = 0; iz < 3; ++iz) {
-                    const float Z = Fz[iz];
-                    const f2 Zs = f2_splat(Z), nZ = f2_splat(-Z);
-                    const f2 R2 = f2_fma(Zs, Zs, XY2);
-                    const f2 inv = f2_rsqrt(R2);
+                    const f2 Zs = f2_splat(Fz[iz]);
+                    f2 inv = f2_rsqrt(f2_fma(Zs, Zs, XY2));
+                    if (grp == 4) inv = inv * keep;
                     const f2 inv2 = inv * inv;
-                    f2 i3 = inv2 * inv;
-                    if (grp == 4) i3 = i3 * keep;
-                    const f2 w = Zs * inv2;
-                    const f2 Gx = f2_fma(m02s, w, g0s), Gy = f2_fma(m12s, w, g1s), Gz = f2_fma(m22s, w, g2s);
-                    accx = f2_fma(f2_fma(Gy, Zs, f2_fma(Gz, nY, m21s)), i3, accx);
-                    accy = f2_fma(f2_fma(Gz, X, Gx * nZ), i3, accy);
-                    accz = f2_fma(f2_fma(Gx, Y, Gy * nX), i3, accz);
+                    const f2 i3 = inv2 * inv;
+                    const f2 i5 = (i3 * inv2) * Zs;
+                    c3 = c3 + i3;
+                    c5 = c5 + i5;
+                    pz = f2_fma(i3, Zs, pz);
+                    qz = f2_fma(i5, Zs, qz);
                   }
+                  px = f2_fma(c3, X, px);
+                  py = f2_fma(c3, Y, py);
+                  qx = f2_fma(c5, X, qx);
+                  qy = f2_fma(c5, Y, qy);
+                  sv = sv + c3;
                 }
               } else {
 #pragma unroll 1
@@ -508,29 +513,21 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
                 const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
                 const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
                 const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
-                const f2 nX = f2_pack(-Xa, -Xb), nY = f2_pack(-Ya, -Yb);
                 const f2 XY2 = f2_fma(X, X, Y * Y);
                 float xy2a, xy2b;
                 f2_unpack(XY2, xy2a, xy2b);
                 // no z image of a column is nearer than its (x, y) distance
                 const bool near_a = test_near && xy2a < fnear2, near_b = test_near && xy2b < fnear2;
+                f2 c3 = f2_splat(0.f), c5 = c3;
 #pragma unroll
                 for (int iz = 0; iz < 3; ++iz) {
                   const float Z = Fz[iz];
-                  const f2 Zs = f2_splat(Z), nZ = f2_splat(-Z);
+                  const f2 Zs = f2_splat(Z);
                   const f2 R2 = f2_fma(Zs, Zs, XY2);
-                  const f2 inv = f2_rsqrt(R2);
-                  const f2 inv2 = inv * inv;
-                  const f2 i3 = inv2 * inv;
-                  const f2 w = Zs * inv2;
-                  const f2 Gx = f2_fma(m02s, w, g0s), Gy = f2_fma(m12s, w, g1s), Gz = f2_fma(m22s, w, g2s);
-                  const f2 cxv = f2_fma(Gy, Zs, f2_fma(Gz, nY, m21s));
-                  const f2 cyv = f2_fma(Gz, X, Gx * nZ);
-                  const f2 czv = f2_fma(Gx, Y, Gy * nX);
+                  float r2a, r2b;
+                  f2_unpack(R2, r2a, r2b);
                   bool on_a = (bits_a >> iz) & 1u, on_b = (bits_b >> iz) & 1u;
                   if ((on_a && near_a) || (on_b && near_b)) {
-                    float r2a, r2b;
-                    f2_unpack(R2, r2a, r2b);
                     // near field: FP64 expansion from the FP64 offsets
                     if (on_a && near_a && r2a < fnear2) {
                       nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixa), cx),
@@ -545,22 +542,42 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
                       on_b = false;
                     }
                   }
-                  float i3a, i3b;
-                  f2_unpack(i3, i3a, i3b);
-                  const f2 i3m = f2_pack(on_a ? i3a : 0.f, on_b ? i3b : 0.f);
-                  accx = f2_fma(cxv, i3m, accx);
-                  accy = f2_fma(cyv, i3m, accy);
-                  accz = f2_fma(czv, i3m, accz);
+                  // images not evaluated here contribute exact zeros
+                  const f2 inv = f2_pack(on_a ? rsqrt_approx(r2a) : 0.f, on_b ? rsqrt_approx(r2b) : 0.f);
+                  const f2 inv2 = inv * inv;
+                  const f2 i3 = inv2 * inv;
+                  const f2 i5 = (i3 * inv2) * Zs;
+                  c3 = c3 + i3;
+                  c5 = c5 + i5;
+                  pz = f2_fma(i3, Zs, pz);
+                  qz = f2_fma(i5, Zs, qz);
                 }
+                px = f2_fma(c3, X, px);
+                py = f2_fma(c3, Y, py);
+                qx = f2_fma(c5, X, qx);
+                qy = f2_fma(c5, Y, qy);
+                sv = sv + c3;
               }
               }
-              float ax0, ax1, ay0, ay1, az0, az1;
-              f2_unpack(accx, ax0, ax1);
-              f2_unpack(accy, ay0, ay1);
-              f2_unpack(accz, az0, az1);
-              ax = ax0 + ax1;
-              ay = ay0 + ay1;
-              az = az0 + az1;
+              float a0, a1;
+              f2_unpack(px, a0, a1);
+              const float Px = a0 + a1;
+              f2_unpack(py, a0, a1);
+              const float Py = a0 + a1;
+              f2_unpack(pz, a0, a1);
+              const float Pz = a0 + a1;
+              f2_unpack(qx, a0, a1);
+              const float Qx = a0 + a1;
+              f2_unpack(qy, a0, a1);
+              const float Qy = a0 + a1;
+              f2_unpack(qz, a0, a1);
+              const float Qz = a0 + a1;
+              f2_unpack(sv, a0, a1);
+              const float S = a0 + a1;
+              // g x P + m x Q + (m21 S, 0, 0), m = (m02, m12, m22)
+              ax = fmaf(g1, Pz, fmaf(-g2, Py, fmaf(m12, Qz, fmaf(-m22, Qy, m21 * S))));
+              ay = fmaf(g2, Px, fmaf(-g0, Pz, fmaf(m22, Qx, -m02 * Qz)));
+              az = fmaf(g0, Py, fmaf(-g1, Px, fmaf(m02, Qy, -m12 * Qx)));
             }
             // the mixed form keeps one sum for the tangle and its images
             nl = nl + mk3(ax, ay, az);
@@ -609,322 +626,6 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
     st3(v_img, k, im);
   }
   // counters: per-warp sums
-  unsigned long long a = n_p2p, b = n_far;
-  for (int off = 16; off > 0; off >>= 1) {
-    a += __shfl_xor_sync(FULL, a, off);
-    b += __shfl_xor_sync(FULL, b, off);
-  }
-  if (lane == 0) {
-    atomicAdd(&counters[0], a);
-    atomicAdd(&counters[1], b);
-    atomicAdd(&counters[2], (unsigned long long)n_iter);
-  }
-}
-
-// ----------------------------------------------------------------------
-// Mixed form, two targets per lane (k_walk_pair).
-//
-// The same traversal and the same exact opening decisions as k_walk_multi,
-// with each lane carrying two neighbouring targets of the key order.  One
-// cell load, one warp-wide minimum and one decode then serve 64 targets,
-// and the two targets' arithmetic forms independent chains.  Their FP32
-// evaluations share packed pairs: half 0 is the first target, half 1 the
-// second, so the 27 images of a cell are 27 packed evaluations with no
-// padding.
-//
-// The 27 image terms of a cell are summed in factored form.  With
-// i3 = |R|^-3 and i5 = R_z |R|^-5 per image, the reference's expansion
-// (g + m R_z / |R|^2) x R i3 + (m21, 0, 0) i3 summed over the images is
-//   g x P + m x Q + (m21 S, 0, 0),  P = sum i3 R,  Q = sum i5 R,  S = sum i3,
-// and since R_x takes one value per x shift (likewise y), P_x and Q_x are
-// sums over the nine (x, y) columns of that shift's offset times the
-// column's sum of i3 (i5).  That is nine lane operations per image instead
-// of sixteen, with the cross products once per cell.
-constexpr int kPairWarps = 4;
-
-#ifndef OV_WALK_PAIR_MIN_BLOCKS
-#define OV_WALK_PAIR_MIN_BLOCKS 4
-#endif
-
-// FP32 offsets r - L s - com per axis and shift, FP64-formed and rounded once
-__device__ __forceinline__ void pair_offsets(const OvParams& P, d3 r, double cx, double cy, double cz,
-                                             float* Fx, float* Fy, float* Fz) {
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    Fx[i] = (float)__dsub_rn(img_coord(r.x, P.L[0], i), cx);
-    Fy[i] = (float)__dsub_rn(img_coord(r.y, P.L[1], i), cy);
-    Fz[i] = (float)__dsub_rn(img_coord(r.z, P.L[2], i), cz);
-  }
-}
-
-// the reference's exact decisions for one target at one opening cell: the
-// images of `m` that accept it (see k_walk_multi)
-__device__ __forceinline__ unsigned pair_decide(const OvParams& P, d3 r, unsigned m, double thr,
-                                                double cx, double cy, double cz) {
-  const double q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)),
-                              wrapped_sq(P, 2, r.z, cz));
-  unsigned pass;
-  if (q0 >= thr * (1.0 + 1e-10)) {
-    pass = m;
-  } else {
-    pass = q0 >= thr ? (1u << kPrimary) : 0u;
-    unsigned rest = m & ~(1u << kPrimary);
-    if (__popc(rest) > kFewImages) {
-      pass |= mac_exact(P, r, cx, cy, cz, thr) & rest;
-    } else {
-      while (rest) {
-        const int c = __ffs(rest) - 1;
-        rest &= rest - 1;
-        const int ix = (c * 57) >> 9, rem = c - 9 * ix, iy = (rem * 11) >> 5, iz = rem - 3 * iy;
-        const double q = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, img_coord(r.x, P.L[0], ix), cx),
-                                             wrapped_sq(P, 1, img_coord(r.y, P.L[1], iy), cy)),
-                                   wrapped_sq(P, 2, img_coord(r.z, P.L[2], iz), cz));
-        if (q >= thr) pass |= 1u << c;
-      }
-    }
-  }
-  return pass & m;
-}
-
-// no image of the target is within the near radius of the centre of mass:
-// an image shifted along an axis has |R|^2 >= that axis offset squared
-__device__ __forceinline__ bool pair_all_far(const float* Fx, const float* Fy, const float* Fz, float n2) {
-  return fmaf(Fz[1], Fz[1], fmaf(Fx[1], Fx[1], Fy[1] * Fy[1])) >= n2 && Fx[0] * Fx[0] >= n2 &&
-         Fx[2] * Fx[2] >= n2 && Fy[0] * Fy[0] >= n2 && Fy[2] * Fy[2] >= n2 && Fz[0] * Fz[0] >= n2 &&
-         Fz[2] * Fz[2] >= n2;
-}
-
-template <int kMinBlocks>
-__global__ void __launch_bounds__(kPairWarps * 32, kMinBlocks)
-    k_walk_pair(OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
-                const double* __restrict__ pos, int n_t, unsigned combos, double near2, double* v_nl,
-                double* v_img, unsigned long long* counters) {
-  // per warp, tree level, target of the pair and lane: images that opened
-  // the parent
-  __shared__ unsigned sh_mask[kPairWarps][kLevelSlots][2][32];
-  const unsigned FULL = 0xffffffffu;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kPairWarps + warp;
-  if (gw * 64 >= n_t) return;   // whole warp out of range
-  int kk[2], nx[2];
-  d3 rr[2], nl[2];
-#pragma unroll
-  for (int t = 0; t < 2; ++t) {
-    const int i = gw * 64 + 2 * lane + t;
-    kk[t] = i < n_t ? (order ? order[i] : i) : -1;
-    const bool live = kk[t] >= 0 && status[kk[t]].x != OV_PINNED && status[kk[t]].x != OV_EMPTY;
-    if (!live) kk[t] = -1;
-    rr[t] = live ? ld3(pos, kk[t]) : mk3(0, 0, 0);
-    nl[t] = mk3(0, 0, 0);
-    nx[t] = live ? 0 : T.n_cells;
-    sh_mask[warp][0][t][lane] = combos;
-  }
-  unsigned n_p2p = 0, n_far = 0, n_iter = 0;
-  const float fnear2 = (float)near2;
-  d3 unused = mk3(0, 0, 0);
-  __syncwarp();
-  for (;;) {
-    const int q = (int)__reduce_min_sync(FULL, (unsigned)min(nx[0], nx[1]));
-    if (q >= T.n_cells) break;
-    const Cell* cp = T.cells + q;
-    if (lane == 0 && q + 1 < T.n_cells) prefetch_l1(cp + 1);
-    const int4 h = *reinterpret_cast<const int4*>(cp);
-    const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);
-    const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]);
-    const int kind = cell_kind(h.w);
-    if (lane == 1 && h.z < T.n_cells) prefetch_l1(T.cells + h.z);
-    const double cx = t0.y, cy = t1.x, cz = t1.y;
-    unsigned pass[2] = {0u, 0u}, p2pm[2] = {0u, 0u};
-    const bool at0 = nx[0] == q, at1 = nx[1] == q;
-    if (at0 || at1) {
-#pragma unroll
-      for (int t = 0; t < 2; ++t) {
-        if (nx[t] != q) continue;
-        const unsigned m = sh_mask[warp][cell_ltop(h.w)][t][lane];
-        unsigned open = 0;
-        if (kind == CELL_LEAF1) {
-          p2p_images<true>(P, m, rr[t], mk3(cx, cy, cz), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x, h.y,
-                           kk[t], near2, nl[t], unused, n_p2p);
-        } else if (kind == CELL_LEAFN) {
-          p2pm[t] = m;
-        } else {
-          pass[t] = pair_decide(P, rr[t], m, t0.x, cx, cy, cz);
-          const unsigned fail = m & ~pass[t];
-          if (kind == CELL_OPEN) open = fail;
-          else if (kind == CELL_OPEN_P2P) p2pm[t] = fail;
-          n_far += __popc(pass[t]);
-        }
-        if (open) sh_mask[warp][cell_lbot(h.w) + 1][t][lane] = open;
-        // each target's next cell strictly increases: the loop ends within n_cells
-        nx[t] = open ? q + 1 : max(h.z, q + 1);
-      }
-      if (pass[0] | pass[1]) {
-        // offsets; a target without accepting images gets harmless ones (its
-        // half is dropped below)
-        float Fx[2][3], Fy[2][3], Fz[2][3];
-#pragma unroll
-        for (int t = 0; t < 2; ++t) {
-          if (pass[t]) {
-            pair_offsets(P, rr[t], cx, cy, cz, Fx[t], Fy[t], Fz[t]);
-          } else {
-#pragma unroll
-            for (int i = 0; i < 3; ++i) Fx[t][i] = Fy[t][i] = Fz[t][i] = 1.0f;
-          }
-        }
-        // an accepting image has |R|^2 >= its wrapped squared distance >=
-        // thr, so a cell whose thr reaches the near radius needs no test
-        const bool test_near = t0.x < near2;
-        bool fast = true;
-#pragma unroll
-        for (int t = 0; t < 2; ++t)
-          fast = fast && (pass[t] == 0 ||
-                          (pass[t] == kAllImages && (!test_near || pair_all_far(Fx[t], Fy[t], Fz[t], fnear2))));
-        f2 X[3], Y[3], Z[3], X2[3], Y2[3], Z2[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) {
-          X[i] = f2_pack(Fx[0][i], Fx[1][i]);
-          Y[i] = f2_pack(Fy[0][i], Fy[1][i]);
-          Z[i] = f2_pack(Fz[0][i], Fz[1][i]);
-          X2[i] = X[i] * X[i];
-          Y2[i] = Y[i] * Y[i];
-          Z2[i] = Z[i] * Z[i];
-        }
-        f2 px, py, pz, qx, qy, qz, s0;
-        if (fast) {
-          // every image of each evaluated target: no masks, no near field
-#pragma unroll
-          for (int col = 0; col < 9; ++col) {
-            const int ix = col / 3, iy = col % 3;
-            const f2 XY2 = X2[ix] + Y2[iy];
-            f2 c3, c5;
-#pragma unroll
-            for (int iz = 0; iz < 3; ++iz) {
-              const f2 inv = f2_rsqrt(XY2 + Z2[iz]);
-              const f2 inv2 = inv * inv;
-              const f2 i3 = inv2 * inv;
-              const f2 i5 = (i3 * inv2) * Z[iz];
-              if (iz == 0) {
-                c3 = i3;
-                c5 = i5;
-              } else {
-                c3 = c3 + i3;
-                c5 = c5 + i5;
-              }
-              if (col == 0 && iz == 0) {
-                pz = i3 * Z[iz];
-                qz = i5 * Z[iz];
-              } else {
-                pz = f2_fma(i3, Z[iz], pz);
-                qz = f2_fma(i5, Z[iz], qz);
-              }
-            }
-            if (col == 0) {
-              px = c3 * X[ix];
-              py = c3 * Y[iy];
-              qx = c5 * X[ix];
-              qy = c5 * Y[iy];
-              s0 = c3;
-            } else {
-              px = f2_fma(c3, X[ix], px);
-              py = f2_fma(c3, Y[iy], py);
-              qx = f2_fma(c5, X[ix], qx);
-              qy = f2_fma(c5, Y[iy], qy);
-              s0 = s0 + c3;
-            }
-          }
-        } else {
-          // per image masks, and near images of either target in FP64
-          px = py = pz = qx = qy = qz = s0 = f2_splat(0.f);
-#pragma unroll 1
-          for (int col = 0; col < 9; ++col) {
-            const unsigned ba = (pass[0] >> (3 * col)) & 7u, bb = (pass[1] >> (3 * col)) & 7u;
-            if (!(ba | bb)) continue;
-            const int ix = (col * 11) >> 5, iy = col - 3 * ix;
-            const f2 Xc = f2_pack(sel3f(ix, Fx[0][0], Fx[0][1], Fx[0][2]), sel3f(ix, Fx[1][0], Fx[1][1], Fx[1][2]));
-            const f2 Yc = f2_pack(sel3f(iy, Fy[0][0], Fy[0][1], Fy[0][2]), sel3f(iy, Fy[1][0], Fy[1][1], Fy[1][2]));
-            const f2 XY2 = f2_fma(Xc, Xc, Yc * Yc);
-            float xya, xyb;
-            f2_unpack(XY2, xya, xyb);
-            // no z image of a column is nearer than its (x, y) distance
-            const bool near_a = test_near && xya < fnear2, near_b = test_near && xyb < fnear2;
-            f2 c3 = f2_splat(0.f), c5 = f2_splat(0.f);
-#pragma unroll
-            for (int iz = 0; iz < 3; ++iz) {
-              bool on_a = (ba >> iz) & 1u, on_b = (bb >> iz) & 1u;
-              const f2 R2 = XY2 + Z2[iz];
-              float ra, rb;
-              f2_unpack(R2, ra, rb);
-              if (on_a && near_a && ra < fnear2) {
-                nl[0] = nl[0] + expansion64_at(cp, mk3(__dsub_rn(img_coord(rr[0].x, P.L[0], ix), cx),
-                                                       __dsub_rn(img_coord(rr[0].y, P.L[1], iy), cy),
-                                                       __dsub_rn(img_coord(rr[0].z, P.L[2], iz), cz)));
-                on_a = false;
-              }
-              if (on_b && near_b && rb < fnear2) {
-                nl[1] = nl[1] + expansion64_at(cp, mk3(__dsub_rn(img_coord(rr[1].x, P.L[0], ix), cx),
-                                                       __dsub_rn(img_coord(rr[1].y, P.L[1], iy), cy),
-                                                       __dsub_rn(img_coord(rr[1].z, P.L[2], iz), cz)));
-                on_b = false;
-              }
-              // images not evaluated here contribute exact zeros
-              const f2 inv = f2_pack(on_a ? rsqrt_approx(ra) : 0.f, on_b ? rsqrt_approx(rb) : 0.f);
-              const f2 inv2 = inv * inv;
-              const f2 i3 = inv2 * inv;
-              const f2 i5 = (i3 * inv2) * Z[iz];
-              c3 = c3 + i3;
-              c5 = c5 + i5;
-              pz = f2_fma(i3, Z[iz], pz);
-              qz = f2_fma(i5, Z[iz], qz);
-            }
-            px = f2_fma(c3, Xc, px);
-            py = f2_fma(c3, Yc, py);
-            qx = f2_fma(c5, Xc, qx);
-            qy = f2_fma(c5, Yc, qy);
-            s0 = s0 + c3;
-          }
-        }
-        // g x P + m x Q + (m21 S, 0, 0), moments pre-scaled by kappa/4pi
-        const float2 q0f = *reinterpret_cast<const float2*>(&cp->f_g[0]);
-        const float2 q1f = *reinterpret_cast<const float2*>(&cp->f_g[2]);
-        const float2 q2f = *reinterpret_cast<const float2*>(&cp->f_m12);
-        const f2 g0 = f2_splat(q0f.x), g1 = f2_splat(q0f.y), g2 = f2_splat(q1f.x);
-        const f2 m02 = f2_splat(q1f.y), m12 = f2_splat(q2f.x), m22 = f2_splat(q2f.y);
-        const f2 m21 = f2_splat(__int_as_float(h.x));
-        const f2 vx = f2_fma(g1, pz, f2_fma(m12, qz, f2_fma(m21, s0, (g2 * py + m22 * qy) * f2_splat(-1.f))));
-        const f2 vy = f2_fma(g2, px, f2_fma(m22, qx, (g0 * pz + m02 * qz) * f2_splat(-1.f)));
-        const f2 vz = f2_fma(g0, py, f2_fma(m02, qy, (g1 * px + m12 * qx) * f2_splat(-1.f)));
-        float ax[2], ay[2], az[2];
-        f2_unpack(vx, ax[0], ax[1]);
-        f2_unpack(vy, ay[0], ay[1]);
-        f2_unpack(vz, az[0], az[1]);
-        // the mixed form keeps one sum for the tangle and its images
-#pragma unroll
-        for (int t = 0; t < 2; ++t)
-          if (pass[t]) nl[t] = nl[t] + mk3(ax[t], ay[t], az[t]);
-      }
-    }
-    ++n_iter;
-    // direct sums over a node range (grain leaves), shared by the warp
-    if (__ballot_sync(FULL, (p2pm[0] | p2pm[1]) != 0)) {
-      const int2 rg = T.cell_range[q];
-      const int end = min(rg.x + rg.y, T.n_nodes);
-      for (int j = max(rg.x, 0); j < end; ++j) {
-        const int2 id = T.nodeids[j];
-        if (!(p2pm[0] | p2pm[1])) continue;
-        const double* nd = T.nodes64 + 6 * (size_t)j;
-        const d3 r1 = mk3(nd[0], nd[1], nd[2]), r2 = mk3(nd[3], nd[4], nd[5]);
-#pragma unroll
-        for (int t = 0; t < 2; ++t)
-          if (p2pm[t]) p2p_images<true>(P, p2pm[t], rr[t], r1, r2, id.x, id.y, kk[t], near2, nl[t], unused, n_p2p);
-      }
-    }
-  }
-#pragma unroll
-  for (int t = 0; t < 2; ++t)
-    if (kk[t] >= 0) {
-      st3(v_nl, kk[t], nl[t]);
-      st3(v_img, kk[t], mk3(0, 0, 0));
-    }
   unsigned long long a = n_p2p, b = n_far;
   for (int off = 16; off > 0; off >>= 1) {
     a += __shfl_xor_sync(FULL, a, off);
@@ -1086,18 +787,7 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
   if (multi) {
     int warps = (n_t + 31) / 32;
     int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
-    static const int pair_form = getenv("OV_WALK_PAIR") ? atoi(getenv("OV_WALK_PAIR")) : 0;
-    if (mixed && pair_form) {
-      const int pwarps = (n_t + 63) / 64;
-      const int pblocks = (pwarps + kPairWarps - 1) / kPairWarps;
-      if (pair_form == 3)
-        k_walk_pair<3><<<pblocks, kPairWarps * 32, 0, s->stream>>>(
-            P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
-      else
-        k_walk_pair<4><<<pblocks, kPairWarps * 32, 0, s->stream>>>(
-            P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
-      OV_LAUNCHED();
-    } else if (mixed) {
+    if (mixed) {
       k_walk_multi<true><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
           P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
       OV_LAUNCHED();

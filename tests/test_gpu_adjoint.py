@@ -177,14 +177,16 @@ def test_interleaved_trajectories_keep_their_own_gradients(adj):
 
 def test_backward_uses_the_forward_runs_vn(adj):
     """Through the C ABI: a velocity call with another vn between forward
-    and backward changes no cotangent."""
+    and backward changes no cotangent (beyond the rounding of the reverse
+    passes' accumulation order, as between checkpoint intervals)."""
     t, a = adj
     g = np.random.default_rng(3).normal(size=(N, 3))
     a.forward(t.pos, VN, 0.0, DT, STEPS, 8)
     xb1, vb1 = a.backward(g)
     a.velocity(t.pos, 5 * VN)
     xb2, vb2 = a.backward(g)
-    assert np.array_equal(xb1, xb2) and np.array_equal(vb1, vb2)
+    assert np.max(np.abs(xb2 - xb1)) <= 1e-13 * np.max(np.abs(xb1))
+    assert np.max(np.abs(vb2 - vb1)) <= 1e-13 * np.max(np.abs(vb1))
 
 
 def test_adjoint_rejects_unsupported_tangles(ov, monkeypatch):
