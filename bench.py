@@ -84,7 +84,7 @@ def parse():
     ap.add_argument("--adjoint-steps", type=int, default=2000)
     ap.add_argument("--shard", action="store_true",
                     help="at one GPU too: the sharded one-tangle run (the default when --gpus > 1)")
-    ap.add_argument("--only", choices=["walk", "direct", "batch", "cfg2", "adjoint", "reconnect"],
+    ap.add_argument("--only", choices=["walk", "walk64", "direct", "batch", "cfg2", "adjoint", "reconnect"],
                     help="run one part alone and print its object (for profiling)")
     ap.add_argument("--independent", action="store_true",
                     help="with --gpus > 1: one independent tangle per rank (weak scaling) as the headline")
@@ -297,6 +297,7 @@ def bh_reference_check(tangle, p, idx, bh64, direct, vs64, n_direct=64):
     ref_bh = np.zeros((m, 3))
     f(C.cast(t.ptr(), C.c_void_p), 0.0, idx.ctypes.data, m, 1, ref_bh.ctypes.data, C.byref(tb))
     t1 = time.perf_counter()
+    t_build = tb.value
     nd = min(n_direct, m)
     ref_direct = np.zeros((nd, 3))
     f(C.cast(t.ptr(), C.c_void_p), 0.0, idx.ctypes.data, nd, 0, ref_direct.ctypes.data, C.byref(tb))
@@ -318,7 +319,7 @@ def bh_reference_check(tangle, p, idx, bh64, direct, vs64, n_direct=64):
         "gpu_bh_fp64_vs_gpu_direct": dist_stats(rel(gpu_bh, gpu_direct)),
         "gpu_bh_fp64_vs_reference_bh": dist_stats(rel(gpu_bh, ref_bh)),
         "gpu_direct_vs_reference_direct": dist_stats(rel(gpu_direct, ref_direct, nd)),
-        "reference_seconds": {"bh_with_build": t1 - t0, "build": tb.value, "direct": t2 - t1},
+        "reference_seconds": {"bh_with_build": t1 - t0, "build": t_build, "direct": t2 - t1},
         "what": ("superfluid velocity vs (local term + flow + Biot-Savart + 26 images) at seeded sample "
                  "nodes; errors are |a - b| / |vs with the direct sum|; the reference's update_velocity "
                  "from oracle/_ref with its own octree (all nodes) and its direct sum (first direct_nodes)"),
@@ -935,7 +936,7 @@ def main():
         raise SystemExit(f"libov_gpu: {lib.ov_last_error_message().decode()}")
     torch.cuda.set_device(local)
     p = params(args.theta)
-    if args.only and args.only != "walk":
+    if args.only and args.only not in ("walk", "walk64"):
         peak32, peak64 = C.c_double(0), C.c_double(0)
         lib.ov_measure_fma_peak(0, C.byref(peak32))
         lib.ov_measure_fma_peak(1, C.byref(peak64))
@@ -959,8 +960,9 @@ def main():
     from openvort_b200.dist import sum_over_ranks
     n_job = int(round(sum_over_ranks(dist, float(n))))
 
-    # ---------------- device-resident timing, mixed precision
-    ov.configure(p, ov.OV_PREC_MIXED)
+    # ---------------- device-resident timing, mixed precision (FP64 for
+    # --only walk64, which profiles the FP64 walk alone)
+    ov.configure(p, ov.OV_PREC_FP64 if args.only == "walk64" else ov.OV_PREC_MIXED)
     st = ov.DeviceState(tangle.copy())
     st.run(0.0, args.dt, args.warmup)
     barrier(dist)
@@ -986,8 +988,8 @@ def main():
     walk_share = rs.bs_kernel_ms / ms_run if ms_run > 0 else None
     build_share = rs.build_ms / ms_run if ms_run > 0 else None
     st.close()
-    if args.only == "walk":
-        print(json.dumps({"only": "walk", "points": n, "ms_per_step": ms_step, "walk_ms": walk_ms,
+    if args.only in ("walk", "walk64"):
+        print(json.dumps({"only": args.only, "points": n, "ms_per_step": ms_step, "walk_ms": walk_ms,
                           "achieved_tflops": achieved, "peak_tflops": peak32.value,
                           "frac": achieved / peak32.value if peak32.value else None,
                           "cell_interactions_per_point": rs.cell_interactions / max(1.0, rs.bs_launches) / n}))

@@ -68,7 +68,10 @@ struct StageOut {
   const double* t_dev;
   int* flag;
   __device__ void operator()(const OvParams& P, int k, bool act, d3 vnl) const {
-    if (!act) return;
+    if (act) finish(P, k, vnl);
+  }
+  // out of line: its registers stay out of the Biot-Savart loop's allocation
+  __device__ __noinline__ void finish(const OvParams& P, int k, d3 vnl) const {
     const Links L{lk, st};
     double d;
     if (!dxi_node(P, L, y, k, d)) {

@@ -17,8 +17,6 @@
 // rounded once) and evaluated two per f32x2 instruction (ov_pair.cuh); near
 // or borderline-colinear pairs fall back to seg_vel64 from the FP64 table;
 // sums accumulate in FP64.
-#include <stdlib.h>
-
 #include <algorithm>
 
 #include "ov_internal.h"
@@ -123,6 +121,9 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
 constexpr int kPB = 128;            // threads per block
 constexpr int kPTgt = kPB * kTT;    // targets per block
 constexpr int kPSrc = 128;          // sources per shared-memory tile (kPSrc / 2 records)
+// interactions (targets x segments x (1 + images)) up to which the mixed
+// direct sum runs in slot order without the key sort
+constexpr double kSlotOrderWork = 2e8;
 
 #ifndef OV_DIRECT_PAIRS_MIN_BLOCKS
 #define OV_DIRECT_PAIRS_MIN_BLOCKS 5
@@ -222,41 +223,38 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_PAIRS_MIN_BLOCKS) k_direct_mixe
   }
 }
 
-// Mixed form in chain order (k_direct_mixed_chain, the sweep in
-// ov_pair.cuh): sources in slot order, each tile's chained segments swept
-// with shared end nodes and the others in the two-source form.  Targets as
-// in k_direct_mixed_pairs (key order, single-rounded offsets), or in slot
-// order with two-float offsets (no key sort needed).
+// Mixed form in chain order for small sums (k_direct_mixed_chain, the sweep
+// in ov_pair.cuh): sources in slot order, each tile's chained segments swept
+// with shared end nodes and the others in the two-source form; targets in
+// slot order with two-float offsets (hi + lo), so R carries ~2 ulps of |R|
+// whatever a block's extent and no key sort is needed.  Measured: on a
+// 4096-point ring an RK4 step takes less than the FP64 form's (the key sort
+// of k_direct_mixed_pairs costs more than its sum there); on the 22.4k-point
+// periodic tangle k_direct_mixed_pairs is faster (18.6 against 27.1 ms).
 static_assert(2 * kCH == kPSrc, "a chain tile is the two-source form's tile");
 
 #ifndef OV_DIRECT_CHAIN_MIN_BLOCKS
 #define OV_DIRECT_CHAIN_MIN_BLOCKS 4
 #endif
-// kTwo: offsets as two floats (hi + lo) for targets and nodes, so R carries
-// ~2 ulps of |R| whatever the block's extent: targets may then come in slot
-// order (order == nullptr) with no key sort.
-template <bool kTwo>
 __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixed_chain(
     OvParams P, SegTab S, int n_src, const double* __restrict__ pos, const int2* __restrict__ tstatus,
-    const int* __restrict__ order, int n_t, int stride, double* __restrict__ part, int chunk) {
-  __shared__ ChainNode<kTwo> sh_node[kCH + 1];
+    int n_t, double* __restrict__ part, int chunk) {
+  __shared__ ChainNode<true> sh_node[kCH + 1];
   __shared__ ChainSeg sh_seg[kCH];
-  __shared__ PairSrc<kTwo> sh_irr[kPSrc / 2];
+  __shared__ PairSrc<true> sh_irr[kPSrc / 2];
   __shared__ int sh_irr_id[kPSrc];
   __shared__ int sh_n_irr;
   const int j = blockIdx.y;   // 0: the tangle itself, j >= 1: image j-1
   const int base = blockIdx.x * kPTgt;
-  // origin: the block's first target in key order; in slot order (two-float
-  // offsets, where the origin costs no accuracy) the coordinate origin,
-  // since a slot there may be EMPTY
-  d3 O = order ? ld3(pos, order[base]) : mk3(0, 0, 0);
-  if (j > 0) O = image_point(P, j - 1, O);
+  // offsets from the coordinate origin (with two-float offsets the origin
+  // costs no accuracy, and a slot may be EMPTY)
+  const d3 O = mk3(0, 0, 0);
   int kk[kTT];
   PairTargets T;
 #pragma unroll
   for (int u = 0; u < kTT; ++u) {
     const int i = base + threadIdx.x + kPB * u;
-    int k = i < n_t ? (order ? order[i] : i) : -1;
+    int k = i < n_t ? i : -1;
     if (k >= 0 && (tstatus[k].x == OV_EMPTY || tstatus[k].x == OV_PINNED)) k = -1;
     kk[u] = k;
     d3 r = O;
@@ -264,7 +262,7 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
       r = ld3(pos, k);
       if (j > 0) r = image_point(P, j - 1, r);
     }
-    set_target(T, u, r.x - O.x, r.y - O.y, r.z - O.z);
+    set_target(T, u, r.x, r.y, r.z);
   }
   double acc[kTT][3];
 #pragma unroll
@@ -320,7 +318,7 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
         off[h][1] = p.y - O.y;
         off[h][2] = p.z - O.z;
       }
-      chain_node_set<kTwo>(sh_node[i], off, valid);
+      chain_node_set<true>(sh_node[i], off, valid);
     }
     // chained segments; the others to the list
     for (int i = threadIdx.x; i < kCH; i += kPB) {
@@ -359,13 +357,13 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
       stage_pair(sh_irr[q], stage_slot(sh_irr_id[2 * q]), 2 * q + 1 < n_irr ? stage_slot(sh_irr_id[2 * q + 1])
                                                                              : src_none());
     __syncthreads();
-    chain_sweep<kTwo>(sh_node, sh_seg, T, acc, f4pi, special);
+    chain_sweep<true>(sh_node, sh_seg, T, acc, f4pi, special);
     // the segments that do not chain, two per record
     {
       f2 b[kTT][3];
 #pragma unroll
       for (int u = 0; u < kTT; ++u) b[u][0] = b[u][1] = b[u][2] = f2_splat(0.f);
-      for (int q = 0; 2 * q < n_irr; ++q) pair_interact<kTwo>(sh_irr[q], T, b, special);
+      for (int q = 0; 2 * q < n_irr; ++q) pair_interact<true>(sh_irr[q], T, b, special);
 #pragma unroll
       for (int u = 0; u < kTT; ++u) {
 #pragma unroll
@@ -381,7 +379,7 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
   for (int u = 0; u < kTT; ++u) {
     const int i = base + threadIdx.x + kPB * u;
     if (i >= n_t) continue;
-    double* o = part + ((size_t)blockIdx.z * gridDim.y + j) * 3 * stride + 3 * (size_t)(order ? order[i] : i);
+    double* o = part + ((size_t)blockIdx.z * gridDim.y + j) * 3 * (size_t)n_t + 3 * (size_t)i;
     const bool act = kk[u] >= 0;
     o[0] = act ? acc[u][0] : 0;
     o[1] = act ? acc[u][1] : 0;
@@ -458,15 +456,13 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
   OvStatsAcc& st = ov_stats_tls();
   int splits = 1;
   if (s->P.precision == OV_PREC_MIXED) {
-    static const int chain_form = getenv("OV_DIRECT_CHAIN") ? atoi(getenv("OV_DIRECT_CHAIN")) : 0;
-    // targets in key order from the tree's sort (timed as the build), or in
-    // slot order for the two-float chain form, which needs no sort
-    const bool slot_order = chain_form == 2;
-    const int* order = nullptr;
+    // small sums: slot order, no key sort (k_direct_mixed_chain); otherwise
+    // key order from the tree's sort (timed as the build)
+    const double work = (double)s->n_targets * (double)s->n_segments * (1 + nimg);
+    const bool slot_order = work <= kSlotOrderWork;
     int n_t = s->n;
     if (!slot_order) {
       if (!ov_tree_build(s, pos, &s->tree)) return false;
-      order = s->tree.perm.as<int>();
       n_t = s->tree.n_nodes;
     }
     if ((slot_order ? s->n_active : s->tree.n_nodes) == 0) {
@@ -478,20 +474,18 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
       return true;
     }
     const int bx = (n_t + kPTgt - 1) / kPTgt;
-    // sources: slots in slot order (chain forms) or the sorted active nodes
-    const int n_src = chain_form ? s->n : s->tree.n_nodes;
+    // sources: every slot in slot order, or the sorted active nodes
+    const int n_src = slot_order ? s->n : s->tree.n_nodes;
     const int chunk = source_chunk(n_src, (long long)bx * (nimg + 1), kPSrc, &splits);
     if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;
     cudaEventRecord(s->ev1, s->stream);
-    if (chain_form == 2) {
-      k_direct_mixed_chain<true><<<dim3(bx, nimg + 1, splits), kPB, 0, s->stream>>>(
-          s->P, S, n_src, pos, s->status.as<int2>(), nullptr, n_t, s->n, s->img_part.as<double>(), chunk);
-    } else if (chain_form) {
-      k_direct_mixed_chain<false><<<dim3(bx, nimg + 1, splits), kPB, 0, s->stream>>>(
-          s->P, S, n_src, pos, s->status.as<int2>(), order, n_t, s->n, s->img_part.as<double>(), chunk);
+    if (slot_order) {
+      k_direct_mixed_chain<<<dim3(bx, nimg + 1, splits), kPB, 0, s->stream>>>(
+          s->P, S, n_src, pos, s->status.as<int2>(), n_t, s->img_part.as<double>(), chunk);
     } else {
       k_direct_mixed_pairs<<<dim3(bx, nimg + 1, splits), kPB, 0, s->stream>>>(
-          s->P, S, n_src, pos, s->status.as<int2>(), order, n_t, s->n, s->img_part.as<double>(), chunk);
+          s->P, S, n_src, pos, s->status.as<int2>(), s->tree.perm.as<int>(), n_t, s->n,
+          s->img_part.as<double>(), chunk);
     }
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());

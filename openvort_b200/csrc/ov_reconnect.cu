@@ -495,7 +495,7 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     const int k = cand[i].x, l = cand[i].y;
     // after a reconnection the reference leaves k's inner loop
     if (k == done_k || tangle->recalculate[k] || tangle->recalculate[l] || linked(k, l)) continue;
-    if (V.pos_of[k] < 0 || V.pos_of[l] < 0) {
+    if (V.pos_of[k] == -1 || V.pos_of[l] == -1) {
       // velocities of the nodes of the next candidates that can still be
       // tested (some may be skipped after later reconnections)
       std::vector<int> batch;
@@ -552,6 +552,27 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     for (int f : flag) tangle->recalculate[f]++;
     ++nrecs;
     done_k = k;
+    // nodes now flagged sit out the rest of the pass: no more velocities for
+    // them (a node whose own links changed may even sit on a zero-length
+    // segment, whose local term is not finite)
+    {
+      std::vector<int> keep;
+      keep.reserve(V.known.size());
+      for (int x : V.known) {
+        if (tangle->recalculate[x]) {
+          V.pos_of[x] = -3;   // retired
+        } else {
+          V.pos_of[x] = (int)keep.size();
+          keep.push_back(x);
+        }
+      }
+      V.known.swap(keep);
+      if (!V.known.empty() &&
+          !ov_cuda_ok(cudaMemcpyAsync(R.known.as<int>(), V.known.data(), sizeof(int) * V.known.size(),
+                                      cudaMemcpyHostToDevice, s->stream),
+                      "cudaMemcpyAsync"))
+        return -ov_last_error();
+    }
     // every known node: the removed and added segments' fields
     SegChange C;
     C.m[0] = changed[0]; C.f[0] = old_fwd[0]; C.sign[0] = -1;
