@@ -20,7 +20,6 @@
 #include <vector>
 
 #include "ov_internal.h"
-#include "ov_node.cuh"
 #include "ov_pair.cuh"
 
 namespace {
@@ -36,10 +35,9 @@ struct BatchView {
 // which every formula here evaluates to exactly zero
 constexpr double kNoSeg = 1.0e4;
 
-// What a Biot-Savart kernel does with a target's sum (inactive targets: EMPTY
-// slots, whose sums are zero).  StoreSums writes v_nl for the per-node
-// kernels that follow; StageOut finishes the RK4 stage of the target in the
-// same launch, so a whole stage is one persistent kernel.
+// What a Biot-Savart kernel does with a target's sum (inactive targets:
+// EMPTY slots, whose sums are zero): v_nl for the per-node kernels that
+// follow.
 struct StoreSums {
   double* v_nl;
   __device__ void operator()(const OvParams&, int k, bool act, d3 v) const {
@@ -47,83 +45,16 @@ struct StoreSums {
   }
 };
 
-// One RK4 stage of target k at the stage positions y: its segment length
-// (dxi), tangent and normal (4-point stencils; the arc lengths formed from
-// positions, since the neighbours' lengths are being written by other
-// blocks), the velocity epilogue at time toff + *t_dev, and then either the
-// next stage's position x0 + h v (euler_step2, src/vortex_dynamics.c:36-52)
-// or, on the last stage, the RK4 combination into x0
-// (src/vortex_dynamics.c:94-112).  The operations are those of k_dxi,
-// k_tangents, k_epilogue, k_euler and k_rk4_combine, so the bits are theirs.
-struct StageOut {
-  const int2* lk;
-  const int2* st;
-  const double* y;
-  const double* x0;
-  double *dxi, *tan, *nrm, *vels, *vs;
-  double* ynext;                     // next stage positions, or null: combine
-  const double *k1, *k2, *k3;        // the last stage's earlier stage velocities
-  double* x0w;
-  double h, dt, toff;
-  const double* t_dev;
-  int* flag;
-  __device__ void operator()(const OvParams& P, int k, bool act, d3 vnl) const {
-    if (act) finish(P, k, vnl);
-  }
-  // out of line: its registers stay out of the Biot-Savart loop's allocation
-  __device__ __noinline__ void finish(const OvParams& P, int k, d3 vnl) const {
-    const Links L{lk, st};
-    double d;
-    if (!dxi_node(P, L, y, k, d)) {
-      atomicOr(flag, 1);
-      return;
-    }
-    dxi[k] = d;
-    d3 t, nn;
-    auto arc = [&](int kk, int dist, double& out) { return arc_length_pos(P, L, y, kk, dist, out); };
-    if (!tangent_node(P, L, y, k, arc, tan, t, nn)) {
-      atomicOr(flag, 1);
-      return;
-    }
-    st3(tan, k, t);
-    st3(nrm, k, nn);
-    d3 v, vsv;
-    const int err = epilogue_node(P, L, toff + *t_dev, y, k, t, nn, vnl, mk3(0, 0, 0), v, vsv);
-    if (err & 1) {
-      atomicOr(flag, 1);
-      return;
-    }
-    if (err) atomicOr(flag, err);
-    st3(vs, k, vsv);
-    st3(vels, k, v);
-    const double vc[3] = {v.x, v.y, v.z};
-    if (ynext) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) ynext[3 * k + c] = x0[3 * k + c] + vc[c] * h;
-    } else {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const int i = 3 * k + c;
-        double mv = k1[i] * (dt / 6);
-        mv += k2[i] * (dt / 3);
-        mv += k3[i] * (dt / 3);
-        mv += vc[c] * (dt / 6);
-        x0w[i] += mv;
-      }
-    }
-  }
-};
-
 // FP64 form: the reference's formula and cut-offs for every pair.  The
 // skip rule of calculate_vs_shift (src/tangle.c:567-569) is implied here:
 // with open boundaries the two segments it skips have an endpoint at the
 // target itself, where the |R| < 1e-8 cut-off returns zero.
-template <int TB, int TS, class Out>
+template <int TB, int TS>
 __global__ void __launch_bounds__(TB) k_batch_bs64(OvParams P, BatchView B,
                                                    const double* __restrict__ pos,
                                                    const int2* __restrict__ links,
                                                    const int2* __restrict__ status,
-                                                   Out out, int* __restrict__ work) {
+                                                   StoreSums out, int* __restrict__ work) {
   __shared__ double sh_r[TS][6];
   __shared__ int sh_item;
   for (;;) {
@@ -176,12 +107,12 @@ __global__ void __launch_bounds__(TB) k_batch_bs64(OvParams P, BatchView B,
 // partial sums over 32 sources are added into FP64 sums.  With open
 // boundaries the two segments the skip rule drops have an endpoint at the
 // target, so they are near and the FP64 cut-off returns zero for them.
-template <int TB, int TS, class Out>
+template <int TB, int TS>
 __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
                                                        const double* __restrict__ pos,
                                                        const int2* __restrict__ links,
                                                        const int2* __restrict__ status,
-                                                       Out out, int* __restrict__ work) {
+                                                       StoreSums out, int* __restrict__ work) {
   static_assert(TS % 32 == 0, "sources per tile");
   __shared__ PairSrc<true> sh[TS / 2];
   __shared__ int sh_item;
@@ -268,12 +199,12 @@ __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
 // Two-float offsets from the coordinate origin (the systems span whole
 // rings, and a slot may be EMPTY); near pairs and pairs at the colinearity
 // cut-off in FP64, FP32 partial sums over 32 segments added into FP64 sums.
-template <int TB, class Out>
+template <int TB>
 __global__ void __launch_bounds__(TB) k_batch_bs_chain(OvParams P, BatchView B,
                                                        const double* __restrict__ pos,
                                                        const int2* __restrict__ links,
                                                        const int2* __restrict__ status,
-                                                       Out out, int* __restrict__ work) {
+                                                       StoreSums out, int* __restrict__ work) {
   __shared__ ChainNode<true> sh_node[kCH + 1];
   __shared__ ChainSeg sh_seg[kCH];
   __shared__ PairSrc<true> sh_irr[kCH];
@@ -432,23 +363,16 @@ __global__ void k_sys_near2(const int* __restrict__ off, const double* __restric
 __global__ void k_advance_time(double* t, double dt) { t[0] += dt; }
 
 using BsKernel = void (*)(OvParams, BatchView, const double*, const int2*, const int2*, StoreSums, int*);
-using StageKernel = void (*)(OvParams, BatchView, const double*, const int2*, const int2*, StageOut, int*);
 
-// the kernel shapes the autotuner chooses from; each in the Biot-Savart-only
-// form (k64, kmixed) and the whole-stage form (s64, smixed)
+// the kernel shapes the autotuner chooses from
 struct Shape {
   int tb, ts;
   BsKernel k64, kmixed;
-  StageKernel s64, smixed;
 };
-#define OV_SHAPE(TB, TS)                                                                        \
-  {TB, TS, k_batch_bs64<TB, TS, StoreSums>, k_batch_bs_mixed<TB, TS, StoreSums>,                \
-   k_batch_bs64<TB, TS, StageOut>, k_batch_bs_mixed<TB, TS, StageOut>}
+#define OV_SHAPE(TB, TS) {TB, TS, k_batch_bs64<TB, TS>, k_batch_bs_mixed<TB, TS>}
 // sources_per_tile 0: the mixed form in chain order (tiles of 128 segments);
 // the FP64 form as with 128
-#define OV_SHAPE_CHAIN(TB)                                                                      \
-  {TB, 0, k_batch_bs64<TB, 128, StoreSums>, k_batch_bs_chain<TB, StoreSums>,                    \
-   k_batch_bs64<TB, 128, StageOut>, k_batch_bs_chain<TB, StageOut>}
+#define OV_SHAPE_CHAIN(TB) {TB, 0, k_batch_bs64<TB, 128>, k_batch_bs_chain<TB>}
 const Shape kShapes[] = {
     OV_SHAPE(64, 64),  OV_SHAPE(64, 128),  OV_SHAPE(64, 256),  OV_SHAPE(128, 64), OV_SHAPE(128, 128),
     OV_SHAPE(128, 256), OV_SHAPE(256, 64), OV_SHAPE(256, 128), OV_SHAPE(256, 256), OV_SHAPE_CHAIN(64),
@@ -506,7 +430,6 @@ bool build_items(ov_batch* b, int tb) {
 // first use (before any graph capture: ov_batch_run calls it first)
 int g_sms = 0;
 int g_occ[kNumShapes][2] = {};
-int g_occ_stage[kNumShapes][2] = {};
 
 bool prepare_shape(int shape, bool mixed) {
   if (!g_sms) {
@@ -521,16 +444,11 @@ bool prepare_shape(int shape, bool mixed) {
     OV_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, mixed ? sh.kmixed : sh.k64, sh.tb, 0));
     if (occ < 1) occ = 1;
   }
-  int& occ_s = g_occ_stage[shape][mixed ? 1 : 0];
-  if (!occ_s) {
-    OV_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, mixed ? sh.smixed : sh.s64, sh.tb, 0));
-    if (occ_s < 1) occ_s = 1;
-  }
   return true;
 }
 
-int grid_for(const ov_batch* b, bool mixed, bool stage = false) {
-  int per_sm = (stage ? g_occ_stage : g_occ)[b->shape][mixed ? 1 : 0];
+int grid_for(const ov_batch* b, bool mixed) {
+  int per_sm = g_occ[b->shape][mixed ? 1 : 0];
   if (per_sm < 1) per_sm = 1;
   if (b->blocks_per_sm > 0) per_sm = std::min(per_sm, b->blocks_per_sm);
   return std::max(1, std::min(b->n_items, g_sms * per_sm));
@@ -552,23 +470,6 @@ bool launch_bs(ov_batch* b, const double* pos, double* v_nl, int* work) {
   const int grid = grid_for(b, mixed);
   k<<<grid, sh.tb, 0, b->s.stream>>>(b->s.P, B, pos, b->s.links.as<int2>(), b->s.status.as<int2>(),
                                      StoreSums{v_nl}, work);
-  OV_LAUNCHED();
-  OV_TRY_CUDA(cudaGetLastError());
-  return true;
-}
-
-// one whole RK4 stage (Biot-Savart sum, geometry, epilogue, stage update) at
-// the stage positions so.y
-bool launch_stage(ov_batch* b, const StageOut& so, int* work) {
-  const Shape& sh = kShapes[b->shape];
-  const bool mixed = b->s.P.precision == OV_PREC_MIXED;
-  if (!build_items(b, item_targets(b->shape, mixed))) return false;
-  if (b->n_items == 0) return true;
-  BatchView B{b->d_off.as<int>(), b->d_items.as<int2>(), b->d_near2.as<double>(), b->n_items};
-  StageKernel k = mixed ? sh.smixed : sh.s64;
-  if (!g_occ_stage[b->shape][mixed ? 1 : 0] && !prepare_shape(b->shape, mixed)) return false;
-  const int grid = grid_for(b, mixed, true);
-  k<<<grid, sh.tb, 0, b->s.stream>>>(b->s.P, B, so.y, b->s.links.as<int2>(), b->s.status.as<int2>(), so, work);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   return true;
@@ -603,59 +504,12 @@ bool enqueue_eval(ov_batch* b, const double* pos, double* dxi, double* tan, doub
 }
 
 // one RK4 step (update_tangle + rk4_step2, src/vortex_dynamics.c:58-117) at
-// time *t_dev, which it then advances by dt
-bool enqueue_step_staged(ov_batch* b, double dt, bool classic);
-
-// One RK4 step as four persistent kernels, one per stage (StageOut): stage
-// q evaluates at Y_q (Y_0 = x0) and writes Y_{q+1} = x0 + h_q k_{q+1}, the
-// stage positions alternating between two buffers since other blocks still
-// read Y_q; the last stage adds the RK4 combination into x0.  Without the
-// Biot-Savart sum (LIA only) the per-node kernels run instead.
+// time *t_dev, which it then advances by dt.  Per stage: the geometry
+// kernels, the persistent Biot-Savart kernel, the epilogue and the stage
+// update.  (One kernel for the whole stage, with each target's geometry,
+// epilogue and update after its sums, measured 74.7 ms per step against
+// 52 ms: the FP64 per-node work ran at the sum kernel's occupancy.)
 bool enqueue_step(ov_batch* b, double dt, bool classic) {
-  ov_state_impl* s = &b->s;
-  if (s->P.lia_only) return enqueue_step_staged(b, dt, classic);
-  double* x0 = s->pos.as<double>();
-  double* ya = s->spos.as<double>();
-  double* yb = s->pos0.as<double>();
-  double* ks[3] = {s->k2.as<double>(), s->k3.as<double>(), s->k4.as<double>()};
-  const double h[3] = {dt / 2, dt / 2, classic ? dt : dt / 2};
-  const double toff[4] = {0.0, dt / 2, dt / 2, dt};
-  int* work = b->d_work.as<int>();
-  OV_TRY_CUDA(cudaMemsetAsync(work, 0, 4 * sizeof(int), s->stream));
-  if (!launch_near2(b, x0)) return false;
-  StageOut so{};
-  so.lk = s->links.as<int2>();
-  so.st = s->status.as<int2>();
-  so.x0 = x0;
-  so.dt = dt;
-  so.t_dev = b->d_time.as<double>();
-  so.flag = s->dflag.as<int>();
-  so.k1 = s->vels.as<double>();
-  so.k2 = ks[0];
-  so.k3 = ks[1];
-  so.x0w = x0;
-  const double* ys[4] = {x0, ya, yb, ya};
-  double* ynext[4] = {ya, yb, ya, nullptr};
-  for (int q = 0; q < 4; ++q) {
-    so.y = ys[q];
-    so.ynext = ynext[q];
-    so.h = q < 3 ? h[q] : 0.0;
-    so.toff = toff[q];
-    so.dxi = q == 0 ? s->dxi.as<double>() : s->sdxi.as<double>();
-    so.tan = q == 0 ? s->tan.as<double>() : s->stan.as<double>();
-    so.nrm = q == 0 ? s->nrm.as<double>() : s->snrm.as<double>();
-    so.vels = q == 0 ? s->vels.as<double>() : ks[q - 1];
-    so.vs = q == 0 ? s->vs.as<double>() : s->svs.as<double>();
-    if (!launch_stage(b, so, work + q)) return false;
-  }
-  k_advance_time<<<1, 1, 0, s->stream>>>(b->d_time.as<double>(), dt);
-  OV_LAUNCHED();
-  OV_TRY_CUDA(cudaGetLastError());
-  return true;
-}
-
-// the same step with per-node kernels between the Biot-Savart sums
-bool enqueue_step_staged(ov_batch* b, double dt, bool classic) {
   ov_state_impl* s = &b->s;
   const int2* st = s->status.as<int2>();
   double* x0 = s->pos.as<double>();

@@ -1,8 +1,7 @@
 // ov_node.cuh - per-node geometry and velocity assembly as device
-// functions: the arc length to the next node, the 4-point tangent and
-// normal stencils, and the epilogue of update_velocity.  The per-node
-// kernels (ov_geom.cu) and the batched RK4 stage kernels (ov_batch.cu) call
-// the same code, so both give the same bits.
+// functions: the segment length to the next node, the 4-point tangent and
+// normal stencils, and the epilogue of update_velocity, for the per-node
+// kernels (ov_geom.cu) and any kernel that must give their bits.
 #pragma once
 
 #include "ov_internal.h"
@@ -38,44 +37,6 @@ __device__ __forceinline__ bool dxi_node(const OvParams& P, const Links& L, cons
   if (!step_node(P, L, pos, k, 1, s1)) return false;
   d3 w = pwrap(P, s0, s1);
   out = norm_ref(s0 - w);
-  return true;
-}
-
-// arc_length (src/tangle.c:208-243) with each segment length formed from
-// the positions by dxi_node instead of read from a stored array: the same
-// values in the same order of summation
-__device__ bool arc_length_pos(const OvParams& P, const Links& L, const double* pos, int k, int dist,
-                               double& out) {
-  double acc = 0;
-  int cur = k, d = dist;
-  for (int it = 0; it < 16 && d != 0; ++it) {
-    bool pin = pinned_any(L.st[cur].x);
-    int2 lk = L.lk[cur];
-    double seg = 0;
-    if (d > 0) {
-      if (lk.x < 0) {
-        if (!pin) return false;
-        d = -d;
-        continue;
-      }
-      if (!dxi_node(P, L, pos, cur, seg)) return false;
-      acc += seg;
-      cur = lk.x;
-      --d;
-    } else {
-      if (lk.y < 0) {
-        if (!pin) return false;
-        d = -d;
-        continue;
-      }
-      if (!dxi_node(P, L, pos, lk.y, seg)) return false;
-      acc += seg;
-      cur = lk.y;
-      ++d;
-    }
-  }
-  if (d != 0) return false;
-  out = acc;
   return true;
 }
 

@@ -11,7 +11,7 @@ import pytest
 
 from openvort_b200 import geometry as G
 from openvort_b200.tangle import Flow, Params
-from oracle.oracle import Ref, have_ref
+from oracle.oracle import Ref, have_ref, rel_err
 
 pytestmark = [pytest.mark.gpu, pytest.mark.skipif(not have_ref(), reason="oracle/_ref not built")]
 
@@ -102,7 +102,9 @@ def test_crossing_rings_match_reference(ov, seed):
     assert ng == nw
     assert np.array_equal(got.links, want.links)
     assert np.array_equal(got.recalc, want.recalc)
-    assert np.allclose(got.vels, want.vels, rtol=1e-12, atol=0)
+    # the velocities update_velocity wrote at each test, per node |dv| / |v|
+    # (a component-wise bound is ill-posed where a component is near zero)
+    assert rel_err(got.vels, want.vels, t.active) < 1e-12
 
 
 @pytest.mark.parametrize("boundary", ["open", "periodic-26"])
@@ -126,7 +128,9 @@ def test_dense_tangle_matches_reference(ov, boundary):
     assert ng == nw
     assert np.array_equal(got.links, want.links)
     assert np.array_equal(got.recalc, want.recalc)
-    assert np.allclose(got.vels, want.vels, rtol=1e-12, atol=0)
+    # the velocities update_velocity wrote at each test, per node |dv| / |v|
+    # (a component-wise bound is ill-posed where a component is near zero)
+    assert rel_err(got.vels, want.vels, t.active) < 1e-12
 
 
 def test_sit_out_flags_are_read_on_entry(ov):
