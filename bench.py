@@ -57,9 +57,11 @@ def _hbm_peak():
 HBM_PEAK, HBM_PEAK_SOURCE = _hbm_peak()
 FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
 # dram__bytes_read.sum + dram__bytes_write.sum of one mixed walk launch per
-# point, from the ncu launch list of this benchmark at 998,438 points (the
-# median of its 9 walk launches, 321.0 MB per launch)
-WALK_DRAM_BYTES_PER_POINT = 321.5
+# point: 53.0 MB over 198,002 points in the ncu capture of this kernel on
+# this generator (profiles/bh_walk_multi_mixed_200k.md), scaled by the points
+WALK_DRAM_BYTES_PER_POINT = 268.0
+WALK_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_walk_multi<mixed> at "
+                       "198,002 points (profiles/bh_walk_multi_mixed_200k.md), 268 B per point x points")
 
 
 def parse():
@@ -1119,6 +1121,7 @@ def main():
             **err,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak32.value, "unit": "TFLOP/s",
                          "frac": achieved / peak32.value if peak32.value else None, "traffic": traffic,
+                         "traffic_source": WALK_TRAFFIC_SOURCE,
                          "kernel": "k_walk_multi<mixed> (Barnes-Hut walk, one traversal per point for all 27 images)",
                          "peak_source": "ov_measure_fma_peak: FP32 FMA burst on this GPU, this run",
                          "flops_per_launch": flops / max(1.0, rs.bs_launches),
