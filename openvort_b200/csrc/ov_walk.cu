@@ -20,8 +20,10 @@
 // segments in FP32 from FP64-formed relative vectors, FP64 sums; the opening
 // test and near segments (|R| < 4 |ds|) in FP64.
 #include <float.h>
+#include <stdlib.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "ov_internal.h"
 #include "ov_pair.cuh"
@@ -328,6 +330,173 @@ __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 
   if (kMixed) nl = nl + mk3(fx, fy, fz);
 }
 
+// Mixed form of one accepted cell at every image in `pass` (a 27-bit mask
+// of the combos 9 (sx+1) + 3 (sy+1) + (sz+1)): FP32 expansions from the FP32
+// moments at R = r - L s - com formed in FP64 and rounded once, summed in
+// factored form and added to nl; images within the near radius in FP64
+// (expansion64_at, added to nl as they come).  m21 is the FP32 m21 moment
+// (the cell header's first word), thr the cell's opening threshold.
+__device__ __forceinline__ void cell_mixed(const OvParams& P, const Cell* cp, float m21, double cx, double cy,
+                                           double cz, double thr, d3 r, unsigned pass, double near2, d3& nl) {
+  const float2 q0f = *reinterpret_cast<const float2*>(&cp->f_g[0]);
+  const float2 q1f = *reinterpret_cast<const float2*>(&cp->f_g[2]);
+  const float2 q2f = *reinterpret_cast<const float2*>(&cp->f_m12);
+  const float g0 = q0f.x, g1 = q0f.y, g2 = q1f.x, m02 = q1f.y, m12 = q2f.x, m22 = q2f.y;
+  float ax, ay, az;
+  {
+    // FP32 copies of the FP64-formed offsets r - L s - com per axis and shift
+    const float Fx[3] = {(float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
+                         (float)__dsub_rn(r.x, cx),
+                         (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx)};
+    const float Fy[3] = {(float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
+                         (float)__dsub_rn(r.y, cy),
+                         (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy)};
+    const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
+                         (float)__dsub_rn(r.z, cz),
+                         (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+    // an accepting image has |R|^2 >= its wrapped squared distance >=
+    // thr, so a cell whose thr reaches the near radius needs no test
+    const bool test_near = thr < near2;
+    const float fnear2 = (float)near2;
+    // two (x, y) columns per packed FP32 pair: columns 2g and 2g + 1
+    // (the last group has column 8 only), their three z images
+    // evaluated side by side (independent chains).  The 27 image
+    // terms are summed in factored form: with i3 = |R|^-3 and
+    // i5 = R_z |R|^-5 per image, the reference's
+    // ((g + m R_z/|R|^2) x R + (m21, 0, 0)) i3 summed over the images
+    // is g x P + m x Q + (m21 S, 0, 0), P = sum i3 R, Q = sum i5 R,
+    // S = sum i3; since R_x and R_y are constant along a column,
+    // P_x, P_y, Q_x, Q_y take each column's sums of i3 and i5 once.
+    f2 px = f2_splat(0.f), py = px, pz = px, qx = px, qy = px, qz = px, sv = px;
+    // All 27 images accept (the usual case: the wrapped opening test
+    // treats every image point like the target) and none is near:
+    // no per-image masks or near-field tests.  An image shifted
+    // along an axis has |R|^2 >= that axis offset squared (FP32
+    // rounding of sums of non-negative terms is monotonic), so when
+    // every shifted offset and the target's own |R|^2 reach the near
+    // radius, no image takes the FP64 path.
+    bool all_far = pass == kAllImages;
+    if (all_far && test_near) {
+      const float X = Fx[1], Y = Fy[1], Z = Fz[1];
+      all_far = fmaf(Z, Z, fmaf(X, X, Y * Y)) >= fnear2 && Fx[0] * Fx[0] >= fnear2 &&
+                Fx[2] * Fx[2] >= fnear2 && Fy[0] * Fy[0] >= fnear2 && Fy[2] * Fy[2] >= fnear2 &&
+                Fz[0] * Fz[0] >= fnear2 && Fz[2] * Fz[2] >= fnear2;
+    }
+    if (all_far) {
+      // unrolled: the column offsets are chosen at compile time
+#pragma unroll
+      for (int grp = 0; grp < 5; ++grp) {
+        const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
+        const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
+        const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
+        const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
+        const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
+        const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
+        const f2 XY2 = f2_fma(X, X, Y * Y);
+        // the last group holds column 8 twice: its second half is dropped
+        const f2 keep = f2_pack(1.f, grp < 4 ? 1.f : 0.f);
+        f2 c3 = f2_splat(0.f), c5 = c3;
+#pragma unroll
+        for (int iz = 0; iz < 3; ++iz) {
+          const f2 Zs = f2_splat(Fz[iz]);
+          f2 inv = f2_rsqrt(f2_fma(Zs, Zs, XY2));
+          if (grp == 4) inv = inv * keep;
+          const f2 inv2 = inv * inv;
+          const f2 i3 = inv2 * inv;
+          const f2 i5 = (i3 * inv2) * Zs;
+          c3 = c3 + i3;
+          c5 = c5 + i5;
+          pz = f2_fma(i3, Zs, pz);
+          qz = f2_fma(i5, Zs, qz);
+        }
+        px = f2_fma(c3, X, px);
+        py = f2_fma(c3, Y, py);
+        qx = f2_fma(c5, X, qx);
+        qy = f2_fma(c5, Y, qy);
+        sv = sv + c3;
+      }
+    } else {
+#pragma unroll 1
+    for (int grp = 0; grp < 5; ++grp) {
+      const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
+      const unsigned bits_a = (pass >> (3 * xa)) & 7u;
+      const unsigned bits_b = grp < 4 ? (pass >> (3 * xb)) & 7u : 0u;
+      if (!(bits_a | bits_b)) continue;
+      const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
+      const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
+      const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
+      const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
+      const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
+      const f2 XY2 = f2_fma(X, X, Y * Y);
+      float xy2a, xy2b;
+      f2_unpack(XY2, xy2a, xy2b);
+      // no z image of a column is nearer than its (x, y) distance
+      const bool near_a = test_near && xy2a < fnear2, near_b = test_near && xy2b < fnear2;
+      f2 c3 = f2_splat(0.f), c5 = c3;
+#pragma unroll
+      for (int iz = 0; iz < 3; ++iz) {
+        const float Z = Fz[iz];
+        const f2 Zs = f2_splat(Z);
+        const f2 R2 = f2_fma(Zs, Zs, XY2);
+        float r2a, r2b;
+        f2_unpack(R2, r2a, r2b);
+        bool on_a = (bits_a >> iz) & 1u, on_b = (bits_b >> iz) & 1u;
+        if ((on_a && near_a) || (on_b && near_b)) {
+          // near field: FP64 expansion from the FP64 offsets
+          if (on_a && near_a && r2a < fnear2) {
+            nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixa), cx),
+                                             __dsub_rn(img_coord(r.y, P.L[1], iya), cy),
+                                             __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
+            on_a = false;
+          }
+          if (on_b && near_b && r2b < fnear2) {
+            nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixb), cx),
+                                             __dsub_rn(img_coord(r.y, P.L[1], iyb), cy),
+                                             __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
+            on_b = false;
+          }
+        }
+        // images not evaluated here contribute exact zeros
+        const f2 inv = f2_pack(on_a ? rsqrt_approx(r2a) : 0.f, on_b ? rsqrt_approx(r2b) : 0.f);
+        const f2 inv2 = inv * inv;
+        const f2 i3 = inv2 * inv;
+        const f2 i5 = (i3 * inv2) * Zs;
+        c3 = c3 + i3;
+        c5 = c5 + i5;
+        pz = f2_fma(i3, Zs, pz);
+        qz = f2_fma(i5, Zs, qz);
+      }
+      px = f2_fma(c3, X, px);
+      py = f2_fma(c3, Y, py);
+      qx = f2_fma(c5, X, qx);
+      qy = f2_fma(c5, Y, qy);
+      sv = sv + c3;
+    }
+    }
+    float a0, a1;
+    f2_unpack(px, a0, a1);
+    const float Px = a0 + a1;
+    f2_unpack(py, a0, a1);
+    const float Py = a0 + a1;
+    f2_unpack(pz, a0, a1);
+    const float Pz = a0 + a1;
+    f2_unpack(qx, a0, a1);
+    const float Qx = a0 + a1;
+    f2_unpack(qy, a0, a1);
+    const float Qy = a0 + a1;
+    f2_unpack(qz, a0, a1);
+    const float Qz = a0 + a1;
+    f2_unpack(sv, a0, a1);
+    const float S = a0 + a1;
+    // g x P + m x Q + (m21 S, 0, 0), m = (m02, m12, m22)
+    ax = fmaf(g1, Pz, fmaf(-g2, Py, fmaf(m12, Qz, fmaf(-m22, Qy, m21 * S))));
+    ay = fmaf(g2, Px, fmaf(-g0, Pz, fmaf(m22, Qx, -m02 * Qz)));
+    az = fmaf(g0, Py, fmaf(-g1, Px, fmaf(m02, Qy, -m12 * Qx)));
+  }
+  // the mixed form keeps one sum for the tangle and its images
+  nl = nl + mk3(ax, ay, az);
+}
+
 // resident blocks per SM the register allocation must allow, measured at
 // 1M points, ms per launch:
 //   mixed 55.5 / 53.4 / 54.6 for 4 / 5 / 6 blocks (128 registers and no
@@ -423,164 +592,7 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
           n_far += __popc(pass);
           // expansion at every accepting image: R = r - L s - com, unwrapped
           if (kMixed) {
-            const float2 q0f = *reinterpret_cast<const float2*>(&cp->f_g[0]);
-            const float2 q1f = *reinterpret_cast<const float2*>(&cp->f_g[2]);
-            const float2 q2f = *reinterpret_cast<const float2*>(&cp->f_m12);
-            const float g0 = q0f.x, g1 = q0f.y, g2 = q1f.x, m02 = q1f.y, m12 = q2f.x, m22 = q2f.y;
-            const float m21 = __int_as_float(h.x);
-            float ax, ay, az;
-            {
-              // FP32 copies of the FP64-formed offsets r - L s - com per axis and shift
-              const float Fx[3] = {(float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
-                                   (float)__dsub_rn(r.x, cx),
-                                   (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx)};
-              const float Fy[3] = {(float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
-                                   (float)__dsub_rn(r.y, cy),
-                                   (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy)};
-              const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
-                                   (float)__dsub_rn(r.z, cz),
-                                   (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
-              // an accepting image has |R|^2 >= its wrapped squared distance >=
-              // thr, so a cell whose thr reaches the near radius needs no test
-              const bool test_near = t0.x < near2;
-              const float fnear2 = (float)near2;
-              // two (x, y) columns per packed FP32 pair: columns 2g and 2g + 1
-              // (the last group has column 8 only), their three z images
-              // evaluated side by side (independent chains).  The 27 image
-              // terms are summed in factored form: with i3 = |R|^-3 and
-              // i5 = R_z |R|^-5 per image, the reference's
-              // ((g + m R_z/|R|^2) x R + (m21, 0, 0)) i3 summed over the images
-              // is g x P + m x Q + (m21 S, 0, 0), P = sum i3 R, Q = sum i5 R,
-              // S = sum i3; since R_x and R_y are constant along a column,
-              // P_x, P_y, Q_x, Q_y take each column's sums of i3 and i5 once.
-              f2 px = f2_splat(0.f), py = px, pz = px, qx = px, qy = px, qz = px, sv = px;
-              // All 27 images accept (the usual case: the wrapped opening test
-              // treats every image point like the target) and none is near:
-              // no per-image masks or near-field tests.  An image shifted
-              // along an axis has |R|^2 >= that axis offset squared (FP32
-              // rounding of sums of non-negative terms is monotonic), so when
-              // every shifted offset and the target's own |R|^2 reach the near
-              // radius, no image takes the FP64 path.
-              bool all_far = pass == kAllImages;
-              if (all_far && test_near) {
-                const float X = Fx[1], Y = Fy[1], Z = Fz[1];
-                all_far = fmaf(Z, Z, fmaf(X, X, Y * Y)) >= fnear2 && Fx[0] * Fx[0] >= fnear2 &&
-                          Fx[2] * Fx[2] >= fnear2 && Fy[0] * Fy[0] >= fnear2 && Fy[2] * Fy[2] >= fnear2 &&
-                          Fz[0] * Fz[0] >= fnear2 && Fz[2] * Fz[2] >= fnear2;
-              }
-              if (all_far) {
-                // unrolled: the column offsets are chosen at compile time
-#pragma unroll
-                for (int grp = 0; grp < 5; ++grp) {
-                  const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
-                  const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
-                  const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
-                  const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
-                  const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
-                  const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
-                  const f2 XY2 = f2_fma(X, X, Y * Y);
-                  // the last group holds column 8 twice: its second half is dropped
-                  const f2 keep = f2_pack(1.f, grp < 4 ? 1.f : 0.f);
-                  f2 c3 = f2_splat(0.f), c5 = c3;
-#pragma unroll
-                  for (int iz = 0; iz < 3; ++iz) {
-                    const f2 Zs = f2_splat(Fz[iz]);
-                    f2 inv = f2_rsqrt(f2_fma(Zs, Zs, XY2));
-                    if (grp == 4) inv = inv * keep;
-                    const f2 inv2 = inv * inv;
-                    const f2 i3 = inv2 * inv;
-                    const f2 i5 = (i3 * inv2) * Zs;
-                    c3 = c3 + i3;
-                    c5 = c5 + i5;
-                    pz = f2_fma(i3, Zs, pz);
-                    qz = f2_fma(i5, Zs, qz);
-                  }
-                  px = f2_fma(c3, X, px);
-                  py = f2_fma(c3, Y, py);
-                  qx = f2_fma(c5, X, qx);
-                  qy = f2_fma(c5, Y, qy);
-                  sv = sv + c3;
-                }
-              } else {
-#pragma unroll 1
-              for (int grp = 0; grp < 5; ++grp) {
-                const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
-                const unsigned bits_a = (pass >> (3 * xa)) & 7u;
-                const unsigned bits_b = grp < 4 ? (pass >> (3 * xb)) & 7u : 0u;
-                if (!(bits_a | bits_b)) continue;
-                const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
-                const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
-                const float Xa = sel3f(ixa, Fx[0], Fx[1], Fx[2]), Xb = sel3f(ixb, Fx[0], Fx[1], Fx[2]);
-                const float Ya = sel3f(iya, Fy[0], Fy[1], Fy[2]), Yb = sel3f(iyb, Fy[0], Fy[1], Fy[2]);
-                const f2 X = f2_pack(Xa, Xb), Y = f2_pack(Ya, Yb);
-                const f2 XY2 = f2_fma(X, X, Y * Y);
-                float xy2a, xy2b;
-                f2_unpack(XY2, xy2a, xy2b);
-                // no z image of a column is nearer than its (x, y) distance
-                const bool near_a = test_near && xy2a < fnear2, near_b = test_near && xy2b < fnear2;
-                f2 c3 = f2_splat(0.f), c5 = c3;
-#pragma unroll
-                for (int iz = 0; iz < 3; ++iz) {
-                  const float Z = Fz[iz];
-                  const f2 Zs = f2_splat(Z);
-                  const f2 R2 = f2_fma(Zs, Zs, XY2);
-                  float r2a, r2b;
-                  f2_unpack(R2, r2a, r2b);
-                  bool on_a = (bits_a >> iz) & 1u, on_b = (bits_b >> iz) & 1u;
-                  if ((on_a && near_a) || (on_b && near_b)) {
-                    // near field: FP64 expansion from the FP64 offsets
-                    if (on_a && near_a && r2a < fnear2) {
-                      nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixa), cx),
-                                                       __dsub_rn(img_coord(r.y, P.L[1], iya), cy),
-                                                       __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
-                      on_a = false;
-                    }
-                    if (on_b && near_b && r2b < fnear2) {
-                      nl = nl + expansion64_at(cp, mk3(__dsub_rn(img_coord(r.x, P.L[0], ixb), cx),
-                                                       __dsub_rn(img_coord(r.y, P.L[1], iyb), cy),
-                                                       __dsub_rn(img_coord(r.z, P.L[2], iz), cz)));
-                      on_b = false;
-                    }
-                  }
-                  // images not evaluated here contribute exact zeros
-                  const f2 inv = f2_pack(on_a ? rsqrt_approx(r2a) : 0.f, on_b ? rsqrt_approx(r2b) : 0.f);
-                  const f2 inv2 = inv * inv;
-                  const f2 i3 = inv2 * inv;
-                  const f2 i5 = (i3 * inv2) * Zs;
-                  c3 = c3 + i3;
-                  c5 = c5 + i5;
-                  pz = f2_fma(i3, Zs, pz);
-                  qz = f2_fma(i5, Zs, qz);
-                }
-                px = f2_fma(c3, X, px);
-                py = f2_fma(c3, Y, py);
-                qx = f2_fma(c5, X, qx);
-                qy = f2_fma(c5, Y, qy);
-                sv = sv + c3;
-              }
-              }
-              float a0, a1;
-              f2_unpack(px, a0, a1);
-              const float Px = a0 + a1;
-              f2_unpack(py, a0, a1);
-              const float Py = a0 + a1;
-              f2_unpack(pz, a0, a1);
-              const float Pz = a0 + a1;
-              f2_unpack(qx, a0, a1);
-              const float Qx = a0 + a1;
-              f2_unpack(qy, a0, a1);
-              const float Qy = a0 + a1;
-              f2_unpack(qz, a0, a1);
-              const float Qz = a0 + a1;
-              f2_unpack(sv, a0, a1);
-              const float S = a0 + a1;
-              // g x P + m x Q + (m21 S, 0, 0), m = (m02, m12, m22)
-              ax = fmaf(g1, Pz, fmaf(-g2, Py, fmaf(m12, Qz, fmaf(-m22, Qy, m21 * S))));
-              ay = fmaf(g2, Px, fmaf(-g0, Pz, fmaf(m22, Qx, -m02 * Qz)));
-              az = fmaf(g0, Py, fmaf(-g1, Px, fmaf(m02, Qy, -m12 * Qx)));
-            }
-            // the mixed form keeps one sum for the tangle and its images
-            nl = nl + mk3(ax, ay, az);
+            cell_mixed(P, cp, __int_as_float(h.x), cx, cy, cz, t0.x, r, pass, near2, nl);
           } else {
             const double g[3] = {cp->y[0], cp->y[1], cp->y[2]};
             const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
@@ -636,6 +648,177 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
     atomicAdd(&counters[1], b);
     atomicAdd(&counters[2], (unsigned long long)n_iter);
   }
+}
+
+
+// ----------------------------------------------------------------------
+// Two-phase mixed walk.  k_walk_multi carries the traversal state and the
+// evaluation's registers at once (16-20 resident warps per SM) and leaves
+// the lanes whose next cell is elsewhere idle.  Here a lean traversal
+// (k_walk_list: the same warp-coherent walk and exact FP64 decisions, no
+// evaluation) writes each target's work in visit order as entries
+// (cell, image mask): the images accepting an expansion, or (cell with
+// kLeafBit) the images summing a leaf's or grain cell's segments directly.
+// k_walk_eval then evaluates every lane's own list with the same per-cell
+// code in the same order, so the sums are k_walk_multi's bit for bit.  A
+// target whose list outgrows the capacity is left to k_walk_multi.
+constexpr int kListWarps = 4;
+constexpr int kLeafBit = 1 << 30;
+
+struct WalkList {
+  int2* e;        // entries of warp w, entry j, lane l at ((w cap + j) 32 + l)
+  int* count;     // per target (sorted index): entries of its walk, beyond cap if it overflowed
+  int* ovf;       // targets (slots) that overflowed, then their number at ovf[n_t]
+  int cap;
+};
+
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kListWarps * 32, kMinBlocks) k_walk_list(
+    OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
+    const double* __restrict__ pos, int n_t, unsigned combos, WalkList W, unsigned long long* counters) {
+  __shared__ unsigned sh_mask[kListWarps][kLevelSlots][32];
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kListWarps + warp;
+  if (gw * 32 >= n_t) return;   // whole warp out of range
+  const int i = gw * 32 + lane;
+  const int k = i < n_t ? (order ? order[i] : i) : -1;
+  const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
+  const d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
+  unsigned* lvl_mask = &sh_mask[warp][0][lane];   // level l at lvl_mask[32 l]
+  lvl_mask[0] = combos;
+  int cnt = 0;
+  unsigned n_far = 0, n_iter = 0;
+  int2* base = W.e + (size_t)gw * W.cap * 32 + lane;
+  auto put = [&](int cell, unsigned mask) {
+    if (cnt < W.cap) base[(size_t)cnt * 32] = make_int2(cell, (int)mask);
+    ++cnt;
+  };
+  int next = live ? 0 : T.n_cells;
+  __syncwarp();
+  for (;;) {
+    const int q = (int)__reduce_min_sync(FULL, (unsigned)next);
+    if (q >= T.n_cells) break;
+    const Cell* cp = T.cells + q;
+    if (lane == 0 && q + 1 < T.n_cells) prefetch_l1(cp + 1);
+    const int4 h = *reinterpret_cast<const int4*>(cp);
+    const int kind = cell_kind(h.w);
+    if (lane == 1 && h.z < T.n_cells) prefetch_l1(T.cells + h.z);
+    if (next == q) {
+      const unsigned m = lvl_mask[32 * cell_ltop(h.w)];
+      unsigned open = 0;
+      if (kind == CELL_LEAF1) {
+        if (h.y != -1) put(q | kLeafBit, m);   // a node without a segment adds nothing
+      } else if (kind == CELL_LEAFN) {
+        put(q | kLeafBit, m);
+      } else {
+        // the opening decisions of k_walk_multi (octree_get_vs, src/octree.c:284-296)
+        const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);
+        const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]);
+        const double cx = t0.y, cy = t1.x, cz = t1.y;
+        unsigned pass;
+        const double q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)),
+                                    wrapped_sq(P, 2, r.z, cz));
+        if (q0 >= t0.x * (1.0 + 1e-10)) {
+          pass = m;
+        } else {
+          pass = q0 >= t0.x ? (1u << kPrimary) : 0u;
+          unsigned rest = m & ~(1u << kPrimary);
+          if (__popc(rest) > kFewImages) {
+            pass |= mac_exact(P, r, cx, cy, cz, t0.x) & rest;
+          } else {
+            while (rest) {
+              const int c = __ffs(rest) - 1;
+              rest &= rest - 1;
+              const int ix = (c * 57) >> 9, rem = c - 9 * ix, iy = (rem * 11) >> 5, iz = rem - 3 * iy;
+              const double qq = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, img_coord(r.x, P.L[0], ix), cx),
+                                                    wrapped_sq(P, 1, img_coord(r.y, P.L[1], iy), cy)),
+                                          wrapped_sq(P, 2, img_coord(r.z, P.L[2], iz), cz));
+              if (qq >= t0.x) pass |= 1u << c;
+            }
+          }
+        }
+        pass &= m;
+        const unsigned fail = m & ~pass;
+        if (kind == CELL_OPEN) open = fail;
+        if (pass) {
+          n_far += __popc(pass);
+          put(q, pass);
+        }
+        if (kind == CELL_OPEN_P2P && fail) put(q | kLeafBit, fail);
+      }
+      if (open) lvl_mask[32 * (cell_lbot(h.w) + 1)] = open;
+      // each lane's next cell strictly increases: the loop ends within n_cells
+      next = open ? q + 1 : max(h.z, q + 1);
+    }
+    ++n_iter;
+  }
+  if (i < n_t) W.count[i] = live ? cnt : 0;
+  const bool over = live && cnt > W.cap;
+  if (over) W.ovf[atomicAdd(&W.ovf[n_t], 1)] = k;
+  // a target left to k_walk_multi is counted there
+  unsigned long long b = over ? 0 : n_far;
+  for (int off = 16; off > 0; off >>= 1) b += __shfl_xor_sync(FULL, b, off);
+  if (lane == 0) {
+    atomicAdd(&counters[1], b);
+    atomicAdd(&counters[2], (unsigned long long)n_iter);
+  }
+}
+
+// Every lane evaluates its own target's entries, in order, with
+// k_walk_multi's per-cell code (cell_mixed, p2p_images).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kListWarps * 32, kMinBlocks) k_walk_eval(
+    OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
+    const double* __restrict__ pos, int n_t, double near2, WalkList W, double* v_nl, double* v_img,
+    unsigned long long* counters) {
+  const unsigned FULL = 0xffffffffu;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * kListWarps + warp;
+  if (gw * 32 >= n_t) return;
+  const int i = gw * 32 + lane;
+  const int k = i < n_t ? (order ? order[i] : i) : -1;
+  const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
+  const int c_all = i < n_t ? W.count[i] : 0;
+  const bool mine = live && c_all <= W.cap;   // overflowed targets: k_walk_multi
+  const int cnt = mine ? c_all : 0;
+  const d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
+  d3 nl = mk3(0, 0, 0), unused = mk3(0, 0, 0);
+  unsigned n_p2p = 0;
+  const int2* base = W.e + (size_t)gw * W.cap * 32 + lane;
+  const int n_max = __reduce_max_sync(FULL, (unsigned)cnt);
+  for (int j = 0; j < n_max; ++j) {
+    if (j >= cnt) continue;
+    const int2 e = base[(size_t)j * 32];
+    const int q = e.x & ~kLeafBit;
+    const unsigned mask = (unsigned)e.y;
+    const Cell* cp = T.cells + q;
+    const int4 h = *reinterpret_cast<const int4*>(cp);
+    const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);
+    const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]);
+    if (!(e.x & kLeafBit)) {
+      cell_mixed(P, cp, __int_as_float(h.x), t0.y, t1.x, t1.y, t0.x, r, mask, near2, nl);
+    } else if (cell_kind(h.w) == CELL_LEAF1) {
+      p2p_images<true>(P, mask, r, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x, h.y, k,
+                       near2, nl, unused, n_p2p);
+    } else {
+      const int2 rg = T.cell_range[q];
+      const int end = min(rg.x + rg.y, T.n_nodes);
+      for (int jn = max(rg.x, 0); jn < end; ++jn) {
+        const int2 id = T.nodeids[jn];
+        const double* nd = T.nodes64 + 6 * (size_t)jn;
+        p2p_images<true>(P, mask, r, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), id.x, id.y, k, near2,
+                         nl, unused, n_p2p);
+      }
+    }
+  }
+  if (mine) {
+    st3(v_nl, k, nl);
+    st3(v_img, k, mk3(0, 0, 0));   // the mixed form keeps one sum for the tangle and its images
+  }
+  unsigned long long a = n_p2p;
+  for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(FULL, a, off);
+  if (lane == 0) atomicAdd(&counters[0], a);
 }
 
 // All nodes: warp w handles sorted targets 32w .. 32w+31, every image.
@@ -735,6 +918,98 @@ static bool read_counters(ov_state_impl* s, OvTree* t) {
   return true;
 }
 
+// exact-size device buffer (the lists are large: no headroom)
+static bool reserve_exact(DevBuf& b, size_t bytes) {
+  if (b.p && b.bytes >= bytes) return true;
+  b.release();
+  if (!ov_cuda_ok(cudaMalloc(&b.p, bytes), "cudaMalloc")) {
+    b.p = nullptr;
+    return false;
+  }
+  b.bytes = bytes;
+  return true;
+}
+
+// The mixed multi-image walk in two phases (k_walk_list, k_walk_eval), and
+// k_walk_multi for the targets whose list outgrew the capacity.  The
+// capacity starts at 2048 entries per target and doubles after a walk in
+// which more than 1% of the targets overflowed, within a quarter of the free
+// device memory; where even 256 entries do not fit, k_walk_multi does it all.
+// entries per target set by ov_set_walk_list_capacity (0: automatic), and
+// the targets of this thread's last mixed walk left to k_walk_multi
+static std::atomic<int> g_list_cap{0};
+static thread_local int tl_last_overflow = 0;
+
+static bool walk_two_phase(ov_state_impl* s, OvTree* t, const OvParams& P, const TreeView& tv,
+                           const int* order, const double* pos, int n_t, unsigned combos, double near2,
+                           double* v_nl, double* v_img, unsigned long long* ctr) {
+  const int warps = (n_t + 31) / 32;
+  const int blocks = (warps + kListWarps - 1) / kListWarps;
+  if (t->list_cap <= 0) t->list_cap = 2048;
+  const int user_cap = g_list_cap.load();
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t per_entry = sizeof(int2) * 32 * (size_t)warps;
+  int cap = user_cap > 0 ? user_cap : t->list_cap;
+  while (cap > 256 && per_entry * cap > t->wlist.bytes && per_entry * cap > free_b / 4) cap /= 2;
+  if (user_cap <= 0 && per_entry * cap > t->wlist.bytes && per_entry * cap > free_b / 4) {
+    k_walk_multi<true><<<(warps + kMultiWarps - 1) / kMultiWarps, kMultiWarps * 32, 0, s->stream>>>(
+        P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
+    OV_LAUNCHED();
+    return true;
+  }
+  if (!reserve_exact(t->wlist, per_entry * cap) || !t->wcount.reserve(sizeof(int) * (size_t)n_t) ||
+      !t->wovf.reserve(sizeof(int) * ((size_t)n_t + 1)))
+    return false;
+  WalkList W{t->wlist.as<int2>(), t->wcount.as<int>(), t->wovf.as<int>(), cap};
+  OV_TRY_CUDA(cudaMemsetAsync(W.ovf + n_t, 0, sizeof(int), s->stream));
+  static const int form = getenv("OV_WALK_LISTS") ? atoi(getenv("OV_WALK_LISTS")) : 0;
+  if (form == 1) {
+    k_walk_list<8><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
+                                                             n_t, combos, W, ctr);
+  } else {
+    k_walk_list<10><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
+                                                              n_t, combos, W, ctr);
+  }
+  OV_LAUNCHED();
+  if (form == 2) {
+    k_walk_eval<5><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
+                                                             n_t, near2, W, v_nl, v_img, ctr);
+  } else if (form == 3) {
+    k_walk_eval<6><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
+                                                             n_t, near2, W, v_nl, v_img, ctr);
+  } else {
+    k_walk_eval<4><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
+                                                             n_t, near2, W, v_nl, v_img, ctr);
+  }
+  OV_LAUNCHED();
+  int n_ovf = 0;
+  OV_TRY_CUDA(cudaMemcpyAsync(&n_ovf, W.ovf + n_t, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  if (n_ovf > 0) {
+    const int ow = (n_ovf + 31) / 32;
+    k_walk_multi<true><<<(ow + kMultiWarps - 1) / kMultiWarps, kMultiWarps * 32, 0, s->stream>>>(
+        P, tv, W.ovf, s->status.as<int2>(), pos, n_ovf, combos, near2, v_nl, v_img, ctr);
+    OV_LAUNCHED();
+  }
+  if (user_cap <= 0 && n_ovf > n_t / 100 && cap == t->list_cap && t->list_cap < (1 << 16)) t->list_cap *= 2;
+  t->last_overflow = n_ovf;
+  tl_last_overflow = n_ovf;
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+extern "C" int ov_set_walk_list_capacity(int entries) {
+  if (entries < 0) {
+    ov_set_error(OV_ERR_INVALID, "ov_set_walk_list_capacity: %d entries", entries);
+    return OV_ERR_INVALID;
+  }
+  g_list_cap.store(entries);
+  return OV_OK;
+}
+
+extern "C" int ov_get_walk_list_overflow(void) { return tl_last_overflow; }
+
 bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own_tree,
                         double* v_nl, double* v_img, int k0, int k_count) {
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(t->counters.as<char>() + 64);
@@ -788,9 +1063,7 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
     int warps = (n_t + 31) / 32;
     int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
     if (mixed) {
-      k_walk_multi<true><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
-          P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
-      OV_LAUNCHED();
+      if (!walk_two_phase(s, t, P, tv, order, pos, n_t, combos, near2, v_nl, v_img, ctr)) return false;
     } else {
       k_walk_multi<false><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
           P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
