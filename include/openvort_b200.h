@@ -547,18 +547,6 @@ int ov_frame_wait(void);
 int ov_frame_info(const char *filename, int *n, double *time);
 int ov_load_frame(const char *filename, struct tangle_state *tangle, double *time);
 
-/* The mixed Barnes-Hut walk runs in two phases: a traversal that lists
- * each target's accepted cells and leaves, then an evaluation of every
- * list at full warp width.  The lists hold `entries` per target (8 bytes
- * each, for every target at once: 8 GB per million targets at 1024);
- * targets with longer walks are evaluated by the one-phase walk, which gives
- * the same bits.  0 (the default): 2048, doubled after a walk in which more
- * than 1% of the targets overflowed, within a quarter of the free device
- * memory.  No counterpart in the reference. */
-int ov_set_walk_list_capacity(int entries);
-/* targets of this thread's last mixed walk that overflowed their list */
-int ov_get_walk_list_overflow(void);
-
 /* Sustained FMA throughput of this GPU in TFLOP/s (2 flops per FMA),
  * fp64 = 0 for FP32, 1 for FP64: the roofline denominator. */
 int ov_measure_fma_peak(int fp64, double *tflops);

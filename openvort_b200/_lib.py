@@ -38,7 +38,7 @@ FUNCTIONS = [
     "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward", "ov_adjoint_generation",
     "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries", "ov_eliminate_small_loops",
     "ov_save_tangle", "ov_save_frame", "ov_state_save_frame", "ov_frame_wait", "ov_frame_info",
-    "ov_load_frame", "ov_check_fast_math", "ov_set_walk_list_capacity", "ov_get_walk_list_overflow",
+    "ov_load_frame", "ov_check_fast_math",
 ]
 DATA = [
     "open_boundaries", "periodic_6", "periodic_18", "periodic_26", "periodic_z_open_xy",
@@ -130,8 +130,6 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
                                            C.c_void_p]),
         "ov_measure_fma_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
         "ov_check_fast_math": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double)]),
-        "ov_set_walk_list_capacity": (C.c_int, [C.c_int]),
-        "ov_get_walk_list_overflow": (C.c_int, []),
         "ov_state_shard": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_size_t]),
         "ov_state_shard_bytes": (C.c_size_t, [C.c_void_p, C.c_int]),
         "ov_state_shard_begin": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.c_double]),

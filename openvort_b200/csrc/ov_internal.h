@@ -94,10 +94,6 @@ struct OvTree {
   DevBuf scratch;
   DevBuf scan_part;     // block sums of the exclusive scans
   DevBuf mom_part;      // per-chunk partial moments of the largest cells
-  // the mixed walk's per-target work lists (k_walk_list / k_walk_eval)
-  DevBuf wlist, wcount, wovf;
-  int list_cap = 0;     // entries per target
-  int last_overflow = 0;   // targets of the last walk left to k_walk_multi
 };
 
 // ---------------------------------------------------------------- state

@@ -745,10 +745,9 @@ void ov_tree_release(OvTree* t) {
   DevBuf* bufs[] = {&t->keys, &t->keys_alt, &t->vals, &t->vals_alt, &t->stop, &t->hist,
                     &t->perm, &t->bnode, &t->cstart_cnt, &t->cbase, &t->cell_of, &t->cells,
                     &t->cell_lm, &t->cell_range, &t->nodes64, &t->nodeids, &t->nodes32, &t->counters,
-                    &t->scratch, &t->scan_part, &t->mom_part, &t->wlist, &t->wcount, &t->wovf};
+                    &t->scratch, &t->scan_part, &t->mom_part};
   for (DevBuf* b : bufs) b->release();
   t->n_nodes = t->n_cells = t->built = 0;
-  t->list_cap = t->last_overflow = 0;
 }
 
 // exclusive scan of v[0..m) in place (block sums in `part`)

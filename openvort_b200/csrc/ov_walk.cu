@@ -20,10 +20,8 @@
 // segments in FP32 from FP64-formed relative vectors, FP64 sums; the opening
 // test and near segments (|R| < 4 |ds|) in FP64.
 #include <float.h>
-#include <stdlib.h>
 
 #include <algorithm>
-#include <atomic>
 
 #include "ov_internal.h"
 #include "ov_pair.cuh"
@@ -497,6 +495,31 @@ __device__ __forceinline__ void cell_mixed(const OvParams& P, const Cell* cp, fl
   nl = nl + mk3(ax, ay, az);
 }
 
+// FP64 form of one accepted cell at every image in `pass`: the reference's
+// expansion (src/octree.c:303-328) at R = r - L s - com, the tangle's own
+// image into nl and the others into im.
+__device__ __forceinline__ void cell_fp64(const OvParams& P, const Cell* cp, double cx, double cy, double cz, d3 r,
+                                          unsigned pass, d3& nl, d3& im) {
+  const double g[3] = {cp->y[0], cp->y[1], cp->y[2]};
+  const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
+  const double Rz[3] = {__dsub_rn(img_coord(r.z, P.L[2], 0), cz), __dsub_rn(r.z, cz),
+                        __dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+#pragma unroll
+  for (int xy = 0; xy < 9; ++xy) {
+    const unsigned bits = (pass >> (3 * xy)) & 7u;
+    if (!bits) continue;
+    const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
+    const double X = __dsub_rn(img_coord(r.x, P.L[0], ix), cx);
+    const double Y = __dsub_rn(img_coord(r.y, P.L[1], iy), cy);
+#pragma unroll
+    for (int iz = 0; iz < 3; ++iz) {
+      if (!((bits >> iz) & 1u)) continue;
+      const d3 v = expansion64(g, mm, mk3(X, Y, Rz[iz]));
+      if (3 * xy + iz == kPrimary) nl = nl + v; else im = im + v;
+    }
+  }
+}
+
 // resident blocks per SM the register allocation must allow, measured at
 // 1M points, ms per launch:
 //   mixed 55.5 / 53.4 / 54.6 for 4 / 5 / 6 blocks (128 registers and no
@@ -594,24 +617,7 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
           if (kMixed) {
             cell_mixed(P, cp, __int_as_float(h.x), cx, cy, cz, t0.x, r, pass, near2, nl);
           } else {
-            const double g[3] = {cp->y[0], cp->y[1], cp->y[2]};
-            const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
-            const double Rz[3] = {__dsub_rn(img_coord(r.z, P.L[2], 0), cz), __dsub_rn(r.z, cz),
-                                  __dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
-#pragma unroll
-            for (int xy = 0; xy < 9; ++xy) {
-              const unsigned bits = (pass >> (3 * xy)) & 7u;
-              if (!bits) continue;
-              const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
-              const double X = __dsub_rn(img_coord(r.x, P.L[0], ix), cx);
-              const double Y = __dsub_rn(img_coord(r.y, P.L[1], iy), cy);
-#pragma unroll
-              for (int iz = 0; iz < 3; ++iz) {
-                if (!((bits >> iz) & 1u)) continue;
-                const d3 v = expansion64(g, mm, mk3(X, Y, Rz[iz]));
-                if (3 * xy + iz == kPrimary) nl = nl + v; else im = im + v;
-              }
-            }
+            cell_fp64(P, cp, cx, cy, cz, r, pass, nl, im);
           }
         }
       }
@@ -650,176 +656,6 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
   }
 }
 
-
-// ----------------------------------------------------------------------
-// Two-phase mixed walk.  k_walk_multi carries the traversal state and the
-// evaluation's registers at once (16-20 resident warps per SM) and leaves
-// the lanes whose next cell is elsewhere idle.  Here a lean traversal
-// (k_walk_list: the same warp-coherent walk and exact FP64 decisions, no
-// evaluation) writes each target's work in visit order as entries
-// (cell, image mask): the images accepting an expansion, or (cell with
-// kLeafBit) the images summing a leaf's or grain cell's segments directly.
-// k_walk_eval then evaluates every lane's own list with the same per-cell
-// code in the same order, so the sums are k_walk_multi's bit for bit.  A
-// target whose list outgrows the capacity is left to k_walk_multi.
-constexpr int kListWarps = 4;
-constexpr int kLeafBit = 1 << 30;
-
-struct WalkList {
-  int2* e;        // entries of warp w, entry j, lane l at ((w cap + j) 32 + l)
-  int* count;     // per target (sorted index): entries of its walk, beyond cap if it overflowed
-  int* ovf;       // targets (slots) that overflowed, then their number at ovf[n_t]
-  int cap;
-};
-
-template <int kMinBlocks>
-__global__ void __launch_bounds__(kListWarps * 32, kMinBlocks) k_walk_list(
-    OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
-    const double* __restrict__ pos, int n_t, unsigned combos, WalkList W, unsigned long long* counters) {
-  __shared__ unsigned sh_mask[kListWarps][kLevelSlots][32];
-  const unsigned FULL = 0xffffffffu;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kListWarps + warp;
-  if (gw * 32 >= n_t) return;   // whole warp out of range
-  const int i = gw * 32 + lane;
-  const int k = i < n_t ? (order ? order[i] : i) : -1;
-  const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
-  const d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
-  unsigned* lvl_mask = &sh_mask[warp][0][lane];   // level l at lvl_mask[32 l]
-  lvl_mask[0] = combos;
-  int cnt = 0;
-  unsigned n_far = 0, n_iter = 0;
-  int2* base = W.e + (size_t)gw * W.cap * 32 + lane;
-  auto put = [&](int cell, unsigned mask) {
-    if (cnt < W.cap) base[(size_t)cnt * 32] = make_int2(cell, (int)mask);
-    ++cnt;
-  };
-  int next = live ? 0 : T.n_cells;
-  __syncwarp();
-  for (;;) {
-    const int q = (int)__reduce_min_sync(FULL, (unsigned)next);
-    if (q >= T.n_cells) break;
-    const Cell* cp = T.cells + q;
-    if (lane == 0 && q + 1 < T.n_cells) prefetch_l1(cp + 1);
-    const int4 h = *reinterpret_cast<const int4*>(cp);
-    const int kind = cell_kind(h.w);
-    if (lane == 1 && h.z < T.n_cells) prefetch_l1(T.cells + h.z);
-    if (next == q) {
-      const unsigned m = lvl_mask[32 * cell_ltop(h.w)];
-      unsigned open = 0;
-      if (kind == CELL_LEAF1) {
-        if (h.y != -1) put(q | kLeafBit, m);   // a node without a segment adds nothing
-      } else if (kind == CELL_LEAFN) {
-        put(q | kLeafBit, m);
-      } else {
-        // the opening decisions of k_walk_multi (octree_get_vs, src/octree.c:284-296)
-        const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);
-        const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]);
-        const double cx = t0.y, cy = t1.x, cz = t1.y;
-        unsigned pass;
-        const double q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)),
-                                    wrapped_sq(P, 2, r.z, cz));
-        if (q0 >= t0.x * (1.0 + 1e-10)) {
-          pass = m;
-        } else {
-          pass = q0 >= t0.x ? (1u << kPrimary) : 0u;
-          unsigned rest = m & ~(1u << kPrimary);
-          if (__popc(rest) > kFewImages) {
-            pass |= mac_exact(P, r, cx, cy, cz, t0.x) & rest;
-          } else {
-            while (rest) {
-              const int c = __ffs(rest) - 1;
-              rest &= rest - 1;
-              const int ix = (c * 57) >> 9, rem = c - 9 * ix, iy = (rem * 11) >> 5, iz = rem - 3 * iy;
-              const double qq = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, img_coord(r.x, P.L[0], ix), cx),
-                                                    wrapped_sq(P, 1, img_coord(r.y, P.L[1], iy), cy)),
-                                          wrapped_sq(P, 2, img_coord(r.z, P.L[2], iz), cz));
-              if (qq >= t0.x) pass |= 1u << c;
-            }
-          }
-        }
-        pass &= m;
-        const unsigned fail = m & ~pass;
-        if (kind == CELL_OPEN) open = fail;
-        if (pass) {
-          n_far += __popc(pass);
-          put(q, pass);
-        }
-        if (kind == CELL_OPEN_P2P && fail) put(q | kLeafBit, fail);
-      }
-      if (open) lvl_mask[32 * (cell_lbot(h.w) + 1)] = open;
-      // each lane's next cell strictly increases: the loop ends within n_cells
-      next = open ? q + 1 : max(h.z, q + 1);
-    }
-    ++n_iter;
-  }
-  if (i < n_t) W.count[i] = live ? cnt : 0;
-  const bool over = live && cnt > W.cap;
-  if (over) W.ovf[atomicAdd(&W.ovf[n_t], 1)] = k;
-  // a target left to k_walk_multi is counted there
-  unsigned long long b = over ? 0 : n_far;
-  for (int off = 16; off > 0; off >>= 1) b += __shfl_xor_sync(FULL, b, off);
-  if (lane == 0) {
-    atomicAdd(&counters[1], b);
-    atomicAdd(&counters[2], (unsigned long long)n_iter);
-  }
-}
-
-// Every lane evaluates its own target's entries, in order, with
-// k_walk_multi's per-cell code (cell_mixed, p2p_images).
-template <int kMinBlocks>
-__global__ void __launch_bounds__(kListWarps * 32, kMinBlocks) k_walk_eval(
-    OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
-    const double* __restrict__ pos, int n_t, double near2, WalkList W, double* v_nl, double* v_img,
-    unsigned long long* counters) {
-  const unsigned FULL = 0xffffffffu;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kListWarps + warp;
-  if (gw * 32 >= n_t) return;
-  const int i = gw * 32 + lane;
-  const int k = i < n_t ? (order ? order[i] : i) : -1;
-  const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
-  const int c_all = i < n_t ? W.count[i] : 0;
-  const bool mine = live && c_all <= W.cap;   // overflowed targets: k_walk_multi
-  const int cnt = mine ? c_all : 0;
-  const d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
-  d3 nl = mk3(0, 0, 0), unused = mk3(0, 0, 0);
-  unsigned n_p2p = 0;
-  const int2* base = W.e + (size_t)gw * W.cap * 32 + lane;
-  const int n_max = __reduce_max_sync(FULL, (unsigned)cnt);
-  for (int j = 0; j < n_max; ++j) {
-    if (j >= cnt) continue;
-    const int2 e = base[(size_t)j * 32];
-    const int q = e.x & ~kLeafBit;
-    const unsigned mask = (unsigned)e.y;
-    const Cell* cp = T.cells + q;
-    const int4 h = *reinterpret_cast<const int4*>(cp);
-    const double2 t0 = *reinterpret_cast<const double2*>(&cp->thr);
-    const double2 t1 = *reinterpret_cast<const double2*>(&cp->x[1]);
-    if (!(e.x & kLeafBit)) {
-      cell_mixed(P, cp, __int_as_float(h.x), t0.y, t1.x, t1.y, t0.x, r, mask, near2, nl);
-    } else if (cell_kind(h.w) == CELL_LEAF1) {
-      p2p_images<true>(P, mask, r, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x, h.y, k,
-                       near2, nl, unused, n_p2p);
-    } else {
-      const int2 rg = T.cell_range[q];
-      const int end = min(rg.x + rg.y, T.n_nodes);
-      for (int jn = max(rg.x, 0); jn < end; ++jn) {
-        const int2 id = T.nodeids[jn];
-        const double* nd = T.nodes64 + 6 * (size_t)jn;
-        p2p_images<true>(P, mask, r, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), id.x, id.y, k, near2,
-                         nl, unused, n_p2p);
-      }
-    }
-  }
-  if (mine) {
-    st3(v_nl, k, nl);
-    st3(v_img, k, mk3(0, 0, 0));   // the mixed form keeps one sum for the tangle and its images
-  }
-  unsigned long long a = n_p2p;
-  for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(FULL, a, off);
-  if (lane == 0) atomicAdd(&counters[0], a);
-}
 
 // All nodes: warp w handles sorted targets 32w .. 32w+31, every image.
 // Targets in `order` (the tree's key order, so a warp's targets are close in
@@ -918,98 +754,6 @@ static bool read_counters(ov_state_impl* s, OvTree* t) {
   return true;
 }
 
-// exact-size device buffer (the lists are large: no headroom)
-static bool reserve_exact(DevBuf& b, size_t bytes) {
-  if (b.p && b.bytes >= bytes) return true;
-  b.release();
-  if (!ov_cuda_ok(cudaMalloc(&b.p, bytes), "cudaMalloc")) {
-    b.p = nullptr;
-    return false;
-  }
-  b.bytes = bytes;
-  return true;
-}
-
-// The mixed multi-image walk in two phases (k_walk_list, k_walk_eval), and
-// k_walk_multi for the targets whose list outgrew the capacity.  The
-// capacity starts at 2048 entries per target and doubles after a walk in
-// which more than 1% of the targets overflowed, within a quarter of the free
-// device memory; where even 256 entries do not fit, k_walk_multi does it all.
-// entries per target set by ov_set_walk_list_capacity (0: automatic), and
-// the targets of this thread's last mixed walk left to k_walk_multi
-static std::atomic<int> g_list_cap{0};
-static thread_local int tl_last_overflow = 0;
-
-static bool walk_two_phase(ov_state_impl* s, OvTree* t, const OvParams& P, const TreeView& tv,
-                           const int* order, const double* pos, int n_t, unsigned combos, double near2,
-                           double* v_nl, double* v_img, unsigned long long* ctr) {
-  const int warps = (n_t + 31) / 32;
-  const int blocks = (warps + kListWarps - 1) / kListWarps;
-  if (t->list_cap <= 0) t->list_cap = 2048;
-  const int user_cap = g_list_cap.load();
-  size_t free_b = 0, total_b = 0;
-  cudaMemGetInfo(&free_b, &total_b);
-  const size_t per_entry = sizeof(int2) * 32 * (size_t)warps;
-  int cap = user_cap > 0 ? user_cap : t->list_cap;
-  while (cap > 256 && per_entry * cap > t->wlist.bytes && per_entry * cap > free_b / 4) cap /= 2;
-  if (user_cap <= 0 && per_entry * cap > t->wlist.bytes && per_entry * cap > free_b / 4) {
-    k_walk_multi<true><<<(warps + kMultiWarps - 1) / kMultiWarps, kMultiWarps * 32, 0, s->stream>>>(
-        P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
-    OV_LAUNCHED();
-    return true;
-  }
-  if (!reserve_exact(t->wlist, per_entry * cap) || !t->wcount.reserve(sizeof(int) * (size_t)n_t) ||
-      !t->wovf.reserve(sizeof(int) * ((size_t)n_t + 1)))
-    return false;
-  WalkList W{t->wlist.as<int2>(), t->wcount.as<int>(), t->wovf.as<int>(), cap};
-  OV_TRY_CUDA(cudaMemsetAsync(W.ovf + n_t, 0, sizeof(int), s->stream));
-  static const int form = getenv("OV_WALK_LISTS") ? atoi(getenv("OV_WALK_LISTS")) : 0;
-  if (form == 1) {
-    k_walk_list<8><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
-                                                             n_t, combos, W, ctr);
-  } else {
-    k_walk_list<10><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
-                                                              n_t, combos, W, ctr);
-  }
-  OV_LAUNCHED();
-  if (form == 2) {
-    k_walk_eval<5><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
-                                                             n_t, near2, W, v_nl, v_img, ctr);
-  } else if (form == 3) {
-    k_walk_eval<6><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
-                                                             n_t, near2, W, v_nl, v_img, ctr);
-  } else {
-    k_walk_eval<4><<<blocks, kListWarps * 32, 0, s->stream>>>(P, tv, order, s->status.as<int2>(), pos,
-                                                             n_t, near2, W, v_nl, v_img, ctr);
-  }
-  OV_LAUNCHED();
-  int n_ovf = 0;
-  OV_TRY_CUDA(cudaMemcpyAsync(&n_ovf, W.ovf + n_t, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
-  if (n_ovf > 0) {
-    const int ow = (n_ovf + 31) / 32;
-    k_walk_multi<true><<<(ow + kMultiWarps - 1) / kMultiWarps, kMultiWarps * 32, 0, s->stream>>>(
-        P, tv, W.ovf, s->status.as<int2>(), pos, n_ovf, combos, near2, v_nl, v_img, ctr);
-    OV_LAUNCHED();
-  }
-  if (user_cap <= 0 && n_ovf > n_t / 100 && cap == t->list_cap && t->list_cap < (1 << 16)) t->list_cap *= 2;
-  t->last_overflow = n_ovf;
-  tl_last_overflow = n_ovf;
-  OV_TRY_CUDA(cudaGetLastError());
-  return true;
-}
-
-extern "C" int ov_set_walk_list_capacity(int entries) {
-  if (entries < 0) {
-    ov_set_error(OV_ERR_INVALID, "ov_set_walk_list_capacity: %d entries", entries);
-    return OV_ERR_INVALID;
-  }
-  g_list_cap.store(entries);
-  return OV_OK;
-}
-
-extern "C" int ov_get_walk_list_overflow(void) { return tl_last_overflow; }
-
 bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own_tree,
                         double* v_nl, double* v_img, int k0, int k_count) {
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(t->counters.as<char>() + 64);
@@ -1063,7 +807,9 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
     int warps = (n_t + 31) / 32;
     int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
     if (mixed) {
-      if (!walk_two_phase(s, t, P, tv, order, pos, n_t, combos, near2, v_nl, v_img, ctr)) return false;
+      k_walk_multi<true><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
+      OV_LAUNCHED();
     } else {
       k_walk_multi<false><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
           P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);

@@ -128,29 +128,6 @@ def test_config2_tangle_bh4_and_direct_vs_reference(ov):
         assert rel_err(mixed.vs[idx], z[key]) < TOL_MIXED, key
 
 
-@pytest.mark.parametrize("name", ["periodic26_bh5", "periodic26_bh3", "open_empty_bh4"])
-def test_two_phase_walk_equals_one_phase(ov, name):
-    """The mixed walk's lists (traversal, then evaluation of every list) give
-    the one-phase walk's bits: with a capacity of 1 entry every target
-    overflows to k_walk_multi, with 40 some do, with the default none."""
-    lib = ov.load()
-    t, p, meta, _ = load(name)
-    out = {}
-    try:
-        for cap in (0, 40, 1):
-            assert lib.ov_set_walk_list_capacity(cap) == 0
-            out[cap] = gpu_update(ov, t, p, meta["time"], precision=1)
-            ovf = lib.ov_get_walk_list_overflow()
-            if cap == 0:
-                assert ovf == 0
-            if cap == 1:
-                assert ovf > 0
-    finally:
-        lib.ov_set_walk_list_capacity(0)
-    assert np.array_equal(out[0].vels, out[1].vels)
-    assert np.array_equal(out[40].vels, out[1].vels)
-
-
 def test_refined_fp64_reciprocals_match_ieee(ov):
     """The direct sum's FP64 1/sqrt(x) and 1/x (hardware approximation plus
     two Newton-Raphson steps) stay within 4 ulps of IEEE sqrt and division
