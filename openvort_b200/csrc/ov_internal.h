@@ -46,7 +46,8 @@ enum { CELL_LEAF1 = 0, CELL_LEAFN = 1, CELL_OPEN = 2, CELL_OPEN_P2P = 3, CELL_OP
 //   bytes   0-15  : a, b, skip, meta = kind | level_top << 8 | level_bot << 16
 //                   LEAF1: a = node slot, b = forward slot
 //                   LEAFN: a = first sorted node, b = node count
-//                   OPEN*: a = FP32 m21 (bit pattern), b unused
+//                   OPEN*: a = FP32 m21 (bit pattern), b = FP32 rounding
+//                   margin of the opening test (bit pattern, mac_margin)
 //                   level_top..level_bot: the octree levels the (chain of)
 //                   cell(s) spans; children start at level_bot + 1
 //   bytes  16-23  : thr, the opening test passes iff the reference-wrapped

@@ -435,6 +435,36 @@ __device__ double mac_threshold(double Lm, double theta) {
   return s;
 }
 
+// Rounding margin E of a cell's opening test for the multi-image walk: the
+// walk decides all of a target's images from the target's own squared
+// distance q0 when q0 >= thr + E (every image passes) or q0 < thr - E (every
+// image fails, where no axis wraps).  Derivation, with u = 2^-53:
+//   - the positions used are within [lo - L/4, hi + L/4] (walk targets are
+//     checked; a non-root cell's centre of mass is a mean of nodes in the box),
+//     so every FP64 value the wrapped distance forms (r -+ L, c -+ L, their
+//     difference) is at most B = 3.5 max_a(|lo_a| + |hi_a|) in magnitude, and
+//     each computed component differs from the exact r_a - c_a by at most
+//     e = 4 u B;
+//   - a computed squared distance q then differs from the exact Q by at most
+//     D(Q) = (2 e sqrt(3 Q) + 3 e^2)(1 + 3.01 u) + 3.01 u Q (three roundings
+//     of the squares and their sums);
+//   - with E = 2 D(4 thr), q0 >= thr + E implies Q > thr + E/2, so each
+//     image (whose exact distance is at least Q) computes q >= thr; q0 < thr - E
+//     and equal exact distances imply each image computes q < thr.
+// 1% slack covers the roundings of this formula and of thr -+ E; the value is
+// rounded up to FP32.  Cells that never pass (thr = DBL_MAX) need no margin;
+// a margin above thr / 2 disables both shortcuts (infinity).
+__device__ float mac_margin(const OvParams& P, double thr) {
+  if (thr == DBL_MAX) return 0.f;
+  double B = 0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) B = fmax(B, fabs(P.lo[a]) + fabs(P.hi[a]));
+  const double u = 0x1p-53, e = 4 * u * 3.5 * B;
+  const double E = 2.02 * ((2 * e * sqrt(12 * thr) + 3 * e * e) * (1 + 3.01 * u) + 12.04 * u * thr);
+  if (!(E < 0.5 * thr)) return __int_as_float(0x7f800000);
+  return __double2float_ru(E);
+}
+
 __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __restrict__ leaf_parent,
                               const CellInfo* __restrict__ info, const unsigned* __restrict__ base,
                               const uint64_t* __restrict__ khi, const uint64_t* __restrict__ klo,
@@ -482,6 +512,7 @@ __global__ void k_write_cells(const BNode* __restrict__ nodes, const int* __rest
     }
     Lm = box_max(lo, hi);
     c.thr = mac_threshold(Lm, P.theta);
+    c.b = __float_as_int(mac_margin(P, c.thr));
     // moments are needed: file the cell by size for the moment kernels,
     // one atomic per class per warp (a list's order does not matter: each
     // cell's moments depend on its own nodes only)

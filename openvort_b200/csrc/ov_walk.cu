@@ -22,6 +22,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <cmath>
 
 #include "ov_internal.h"
 #include "ov_pair.cuh"
@@ -228,11 +229,33 @@ constexpr unsigned kAllImages = (1u << 27) - 1;
 constexpr int kLevelSlots = 34;
 constexpr int kMultiWarps = 4;
 
+// Parameters of the walk's shortcut decisions (every image from the
+// target's own distance): on = no image shifts along a non-periodic axis
+// (whose images may lie nearer than the target); hw[a] = the largest
+// |c - r| along axis a at which every image's wrap still undoes its shift
+// (half a box less a rounding allowance; DBL_MAX on axes without shifts).
+struct ImageShortcut {
+  double hw[3];
+  int on;
+};
+
 // wrapped component u and its square for one image coordinate v
 __device__ __forceinline__ double wrapped_sq(const OvParams& P, int a, double v, double c) {
   double cc = c;
   if (P.periodic[a]) {
     double d = __dsub_rn(c, v);
+    if (d > P.L[a] * 0.5) cc = __dsub_rn(c, P.L[a]);
+    else if (d < -P.L[a] * 0.5) cc = __dadd_rn(c, P.L[a]);
+  }
+  double u = __dsub_rn(v, cc);
+  return __dmul_rn(u, u);
+}
+
+// the same with the unwrapped difference c - v in d (every axis)
+__device__ __forceinline__ double wrapped_sq_d(const OvParams& P, int a, double v, double c, double& d) {
+  double cc = c;
+  d = __dsub_rn(c, v);
+  if (P.periodic[a]) {
     if (d > P.L[a] * 0.5) cc = __dsub_rn(c, P.L[a]);
     else if (d < -P.L[a] * 0.5) cc = __dadd_rn(c, P.L[a]);
   }
@@ -538,8 +561,8 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
                                                            : OV_WALK_MULTI_MIN_BLOCKS_FP64)
     k_walk_multi(
     OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
-    const double* __restrict__ pos, int n_t, unsigned combos, double near2, double* v_nl,
-    double* v_img, unsigned long long* counters) {
+    const double* __restrict__ pos, int n_t, unsigned combos, ImageShortcut S, double near2,
+    double* v_nl, double* v_img, unsigned long long* counters) {
   __shared__ unsigned sh_mask[kMultiWarps][kLevelSlots][32];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -549,6 +572,14 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
   const int k = i < n_t ? (order ? order[i] : i) : -1;
   const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
   const d3 r = live ? ld3(pos, k) : mk3(0, 0, 0);
+  // the shortcuts' bound on rounding holds for targets within a quarter box
+  // of the box (a node further out takes every decision in full)
+  bool sane = S.on;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double v = a == 0 ? r.x : (a == 1 ? r.y : r.z);
+    sane = sane && v >= P.lo[a] - 0.25 * P.L[a] && v <= P.hi[a] + 0.25 * P.L[a];
+  }
   unsigned* lvl_mask = &sh_mask[warp][0][lane];   // level l at lvl_mask[32 l]
   lvl_mask[0] = combos;
   d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
@@ -577,16 +608,26 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
       } else {
         // opening test per image (octree_get_vs, src/octree.c:284-296)
         const double cx = t0.y, cy = t1.x, cz = t1.y;
-        // Every image point is at least as far from the centre of mass as the
-        // target itself, per axis, in exact arithmetic.  The FP64 rounding of
-        // a wrapped square is at most ~2e-16 L per component, i.e. below
-        // 1e-11 of thr for the smallest cells, so when the target passes with
-        // a 1e-10 margin every image passes too.  Otherwise all 27 decisions.
+        // Per axis, an image point's exact wrapped distance to the centre
+        // of mass is at least the target's, and equal to it when the
+        // target's unwrapped difference c - r is below half a box (the
+        // image's single wrap then undoes its shift).  The cell's margin E
+        // (mac_margin) bounds the FP64 rounding of every image's squared
+        // distance, so when the target's q0 passes by E every image passes,
+        // and when q0 fails by E with no axis near half a box every image
+        // fails.  Otherwise (and at the root, whose centre of mass may lie
+        // outside the box) all decisions are taken in full.
         unsigned pass;
-        const double q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)),
-                                    wrapped_sq(P, 2, r.z, cz));
-        if (q0 >= t0.x * (1.0 + 1e-10)) {
+        double dx, dy, dz;
+        const double q0 = __dadd_rn(__dadd_rn(wrapped_sq_d(P, 0, r.x, cx, dx), wrapped_sq_d(P, 1, r.y, cy, dy)),
+                                    wrapped_sq_d(P, 2, r.z, cz, dz));
+        const double E = (double)__int_as_float(h.y);
+        const bool shortcut = sane && q > 0;
+        if (shortcut && q0 >= t0.x + E) {
           pass = m;
+        } else if (shortcut && q0 < t0.x - E && fabs(dx) <= S.hw[0] && fabs(dy) <= S.hw[1] &&
+                   fabs(dz) <= S.hw[2]) {
+          pass = 0;
         } else {
           // q0 is the target's own decision in mac_exact's operations; the
           // other images still open here are few below the top levels, so
@@ -802,17 +843,35 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
     combos |= bit;
   }
   const double near2 = s->P.near2;
+  // shortcut parameters: see ImageShortcut and mac_margin (the rounding
+  // allowance 8 u B with B the bound on magnitudes of mac_margin)
+  ImageShortcut sc;
+  {
+    double B = 0;
+    for (int a = 0; a < 3; ++a) B = std::max(B, std::fabs(P.lo[a]) + std::fabs(P.hi[a]));
+    const double allowance = 8 * 0x1p-53 * 3.5 * B;
+    sc.on = 1;
+    for (int a = 0; a < 3; ++a) {
+      bool shifted = false;
+      for (int c = 0; c < kCombos; ++c) {
+        const int sa = a == 0 ? c / 9 : (a == 1 ? (c / 3) % 3 : c % 3);
+        if (((combos >> c) & 1u) && sa != 1) shifted = true;
+      }
+      if (shifted && !P.periodic[a]) sc.on = 0;
+      sc.hw[a] = shifted ? 0.5 * P.L[a] - allowance : DBL_MAX;
+    }
+  }
   cudaEventRecord(s->ev1, s->stream);
   if (multi) {
     int warps = (n_t + 31) / 32;
     int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
     if (mixed) {
       k_walk_multi<true><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
-          P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, sc, near2, v_nl, v_img, ctr);
       OV_LAUNCHED();
     } else {
       k_walk_multi<false><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
-          P, tv, order, s->status.as<int2>(), pos, n_t, combos, near2, v_nl, v_img, ctr);
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, sc, near2, v_nl, v_img, ctr);
       OV_LAUNCHED();
     }
   } else {
