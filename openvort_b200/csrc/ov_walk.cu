@@ -351,6 +351,107 @@ __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 
   if (kMixed) nl = nl + mk3(fx, fy, fz);
 }
 
+// Mixed form of one segment r1 -> r2 at every image in `mask` with many
+// images: the images' offsets R = r1 - (r - L s) per axis and shift are
+// formed in FP64 and rounded once, and two (x, y) image columns share each
+// packed FP32 pair (columns 2g and 2g + 1, their three z images one after
+// the other), as in cell_mixed.  Per image, with d = r2 - r1, a = |R|,
+// b = |R + d|, u = 1/(ab), w = u / (1 + R.(R + d) u):
+//   v = kappa/4pi (1/a + 1/b) w (R x d),   1 - cos = |R x d|^2 u w
+// (the reference's segment formula, src/tangle.c:486-517, and its
+// colinearity cut-off, zero inside it).  R x d, R.d and |R|^2 share their
+// x and y parts along a column.  Images nearer than the far radius, or
+// within 2.5e-3 of the cut-off, take the FP64 formula afterwards.  The skip
+// rule (calculate_vs_shift, src/tangle.c:567-569) drops the tangle's own
+// image for the target's own segments.
+__device__ __forceinline__ void p2p_mixed_columns(const OvParams& P, unsigned mask, d3 r, d3 r1, d3 r2,
+                                                  int id, int fw, int skip, double near2, d3& nl,
+                                                  unsigned& n_p2p) {
+  if (fw == -1) return;
+  if (id == skip || fw == skip) mask &= ~(1u << kPrimary);
+  n_p2p += __popc(mask);
+  const d3 ds = r2 - r1;
+  const double ds2 = dot3(ds, ds);
+  const float far2 = (float)fmax(16.0 * ds2, near2);
+  const float dx = (float)ds.x, dy = (float)ds.y, dz = (float)ds.z;
+  const f2 Dx = f2_splat(dx), Dz = f2_splat(dz), nDy = f2_splat(-dy);
+  const f2 D2 = f2_splat(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
+  const f2 one = f2_splat(1.0f), two = f2_splat(2.0f);
+  // FP32 copies of r1 - (r - L s) per axis and shift
+  const float Fx[3] = {(float)__dsub_rn(r1.x, img_coord(r.x, P.L[0], 0)), (float)__dsub_rn(r1.x, r.x),
+                       (float)__dsub_rn(r1.x, img_coord(r.x, P.L[0], 2))};
+  const float Fy[3] = {(float)__dsub_rn(r1.y, img_coord(r.y, P.L[1], 0)), (float)__dsub_rn(r1.y, r.y),
+                       (float)__dsub_rn(r1.y, img_coord(r.y, P.L[1], 2))};
+  const float Fz[3] = {(float)__dsub_rn(r1.z, img_coord(r.z, P.L[2], 0)), (float)__dsub_rn(r1.z, r.z),
+                       (float)__dsub_rn(r1.z, img_coord(r.z, P.L[2], 2))};
+  f2 bx = f2_splat(0.f), by = bx, bz = bx;
+  unsigned special = 0;   // images left to the FP64 formula
+#pragma unroll
+  for (int grp = 0; grp < 5; ++grp) {
+    const int xa = 2 * grp, xb = grp < 4 ? xa + 1 : xa;
+    const unsigned bits_a = (mask >> (3 * xa)) & 7u;
+    const unsigned bits_b = grp < 4 ? (mask >> (3 * xb)) & 7u : 0u;
+    if (!(bits_a | bits_b)) continue;
+    const int ixa = (xa * 11) >> 5, iya = xa - 3 * ixa;
+    const int ixb = (xb * 11) >> 5, iyb = xb - 3 * ixb;
+    const f2 X = f2_pack(sel3f(ixa, Fx[0], Fx[1], Fx[2]), sel3f(ixb, Fx[0], Fx[1], Fx[2]));
+    const f2 Y = f2_pack(sel3f(iya, Fy[0], Fy[1], Fy[2]), sel3f(iyb, Fy[0], Fy[1], Fy[2]));
+    const f2 XY2 = f2_fma(X, X, Y * Y);
+    const f2 XYd = f2_fma(X, Dx, Y * f2_splat(dy));
+    const f2 Ydz = Y * Dz, mXdz = X * f2_splat(-dz);
+    const f2 Cz = f2_fma(X, f2_splat(dy), Y * f2_splat(-dx));
+    const f2 Cz2 = Cz * Cz;
+#pragma unroll
+    for (int iz = 0; iz < 3; ++iz) {
+      const f2 Zs = f2_splat(Fz[iz]);
+      const f2 R2 = f2_fma(Zs, Zs, XY2);
+      const f2 Rd = f2_fma(Zs, Dz, XYd);
+      const f2 Q2 = f2_fma(two, Rd, R2 + D2);
+      const f2 ia = f2_rsqrt(R2), ib = f2_rsqrt(Q2);
+      const f2 u = ia * ib;
+      const f2 w = u * f2_rcp(f2_fma(R2 + Rd, u, one));
+      const f2 s = (ia + ib) * w;
+      const f2 Cx = f2_fma(Zs, nDy, Ydz);
+      const f2 Cy = f2_fma(Zs, Dx, mXdz);
+      const f2 tc = f2_fma(Cy, Cy, f2_fma(Cx, Cx, Cz2)) * (u * w);   // 1 - cos
+      float tc0, tc1, r20, r21, s0, s1;
+      f2_unpack(tc, tc0, tc1);
+      f2_unpack(R2, r20, r21);
+      f2_unpack(s, s0, s1);
+      const bool in0 = (bits_a >> iz) & 1u, in1 = (bits_b >> iz) & 1u;
+      const bool far0 = r20 >= far2, far1 = r21 >= far2;
+      const bool ok0 = in0 && far0 && tc0 > kColHi, ok1 = in1 && far1 && tc1 > kColHi;
+      // colinear (zero), masked-out and FP64 images add nothing here
+      const f2 sk = f2_pack(ok0 ? s0 : 0.f, ok1 ? s1 : 0.f);
+      bx = f2_fma(Cx, sk, bx);
+      by = f2_fma(Cy, sk, by);
+      bz = f2_fma(Cz, sk, bz);
+      if (in0 && !ok0 && !(far0 && tc0 < kColLo)) special |= 1u << (3 * xa + iz);
+      if (in1 && !ok1 && !(far1 && tc1 < kColLo)) special |= 1u << (3 * xb + iz);
+    }
+  }
+  float lo, hi;
+  const float f4 = (float)P.f4pi;
+  f2_unpack(bx, lo, hi);
+  const float fx = f4 * (lo + hi);
+  f2_unpack(by, lo, hi);
+  const float fy = f4 * (lo + hi);
+  f2_unpack(bz, lo, hi);
+  const float fz = f4 * (lo + hi);
+  nl = nl + mk3(fx, fy, fz);
+#pragma unroll 1
+  while (special) {
+    const int c = __ffs(special) - 1;
+    special &= special - 1;
+    const int ix = (c * 57) >> 9, rem = c - 9 * ix, iy = (rem * 11) >> 5, iz = rem - 3 * iy;
+    nl = nl + seg64_at(P.f4pi, r1, r2,
+                       mk3(img_coord(r.x, P.L[0], ix), img_coord(r.y, P.L[1], iy), img_coord(r.z, P.L[2], iz)));
+  }
+}
+
+// images at which a segment is evaluated by columns rather than one by one
+constexpr int kColumnImages = 8;
+
 // Mixed form of one accepted cell at every image in `pass` (a 27-bit mask
 // of the combos 9 (sx+1) + 3 (sy+1) + (sz+1)): FP32 expansions from the FP32
 // moments at R = r - L s - com formed in FP64 and rounded once, summed in
@@ -601,8 +702,12 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
       const unsigned m = lvl_mask[32 * cell_ltop(h.w)];
       unsigned open = 0;
       if (kind == CELL_LEAF1) {
-        p2p_images<kMixed>(P, m, r, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x,
-                           h.y, k, near2, nl, im, n_p2p);
+        if (kMixed && __popc(m) >= kColumnImages)
+          p2p_mixed_columns(P, m, r, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x, h.y, k,
+                            near2, nl, n_p2p);
+        else
+          p2p_images<kMixed>(P, m, r, mk3(t0.y, t1.x, t1.y), mk3(cp->y[0], cp->y[1], cp->y[2]), h.x,
+                             h.y, k, near2, nl, im, n_p2p);
       } else if (kind == CELL_LEAFN) {
         p2p_mask = m;
       } else {
@@ -675,8 +780,12 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
         const int2 id = T.nodeids[j];
         if (!p2p_mask) continue;
         const double* nd = T.nodes64 + 6 * (size_t)j;
-        p2p_images<kMixed>(P, p2p_mask, r, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), id.x,
-                           id.y, k, near2, nl, im, n_p2p);
+        if (kMixed && __popc(p2p_mask) >= kColumnImages)
+          p2p_mixed_columns(P, p2p_mask, r, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), id.x, id.y,
+                            k, near2, nl, n_p2p);
+        else
+          p2p_images<kMixed>(P, p2p_mask, r, mk3(nd[0], nd[1], nd[2]), mk3(nd[3], nd[4], nd[5]), id.x,
+                             id.y, k, near2, nl, im, n_p2p);
       }
     }
   }
