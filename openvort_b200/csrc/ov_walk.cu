@@ -646,12 +646,13 @@ __device__ __forceinline__ void cell_fp64(const OvParams& P, const Cell* cp, dou
 
 // resident blocks per SM the register allocation must allow, measured at
 // 1M points, ms per launch:
-//   mixed 55.5 / 53.4 / 54.6 for 4 / 5 / 6 blocks (128 registers and no
-//   spills, 96 and 100 bytes spilled, 80 and 196 bytes spilled): the extra
-//   warps hide more of the latency than the spills cost
-//   FP64 95.2 / 85.9 / 82.3 for 4 / 5 / 6 blocks
+//   mixed 47.6 / 40.6 / 43.8 / 44.8 for 3 / 4 / 5 / 6 blocks (136 and 128
+//   registers without spills, 96 registers and 56 bytes spilled, 80
+//   registers and 272 bytes spilled)
+//   FP64 93.4 / 84.7 / 81.0 for 4 / 5 / 6 blocks (102 and 96 registers
+//   without spills, 80 registers and 84 bytes spilled)
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_MIXED
-#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 5
+#define OV_WALK_MULTI_MIN_BLOCKS_MIXED 4
 #endif
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_FP64
 #define OV_WALK_MULTI_MIN_BLOCKS_FP64 6
