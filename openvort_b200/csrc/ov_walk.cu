@@ -344,7 +344,9 @@ __device__ __forceinline__ void p2p_images(const OvParams& P, unsigned mask, d3 
       nl = nl + seg64_at(P.f4pi, r1, r2, t);
       continue;
     }
-    const d3 v = seg64_at(P.f4pi, r1, r2, t);
+    // the reference's formula with Newton-refined reciprocals (its own
+    // operations near the cut-offs), as the FP64 direct sum
+    const d3 v = seg_vel64_nr(P.f4pi, r1, r2, ds, t);
     if (c == kPrimary) nl = nl + v;
     else im = im + v;
   }
@@ -620,28 +622,55 @@ __device__ __forceinline__ void cell_mixed(const OvParams& P, const Cell* cp, fl
 }
 
 // FP64 form of one accepted cell at every image in `pass`: the reference's
-// expansion (src/octree.c:303-328) at R = r - L s - com, the tangle's own
-// image into nl and the others into im.
+// expansion (src/octree.c:303-328) at R = r - L s - com.  The tangle's own
+// image goes into nl as one evaluation; the other images are summed in
+// factored form into im, as in cell_mixed: with i3 = |R|^-3 and
+// i5 = R_z |R|^-5 per image, the sum of ((g + m R_z/|R|^2) x R + (m21, 0, 0)) i3
+// is g x P + m x Q + (m21 S, 0, 0), P = sum i3 R, Q = sum i5 R, S = sum i3.
 __device__ __forceinline__ void cell_fp64(const OvParams& P, const Cell* cp, double cx, double cy, double cz, d3 r,
                                           unsigned pass, d3& nl, d3& im) {
   const double g[3] = {cp->y[0], cp->y[1], cp->y[2]};
   const double mm[4] = {cp->m[0], cp->m[1], cp->m[2], cp->m[3]};
   const double Rz[3] = {__dsub_rn(img_coord(r.z, P.L[2], 0), cz), __dsub_rn(r.z, cz),
                         __dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
+  if (pass & (1u << kPrimary))
+    nl = nl + expansion64(g, mm, mk3(__dsub_rn(r.x, cx), __dsub_rn(r.y, cy), Rz[1]));
+  const unsigned rest = pass & ~(1u << kPrimary);
+  if (!rest) return;
+  double px = 0, py = 0, pz = 0, qx = 0, qy = 0, qz = 0, sv = 0;
 #pragma unroll
   for (int xy = 0; xy < 9; ++xy) {
-    const unsigned bits = (pass >> (3 * xy)) & 7u;
+    const unsigned bits = (rest >> (3 * xy)) & 7u;
     if (!bits) continue;
     const int ix = (xy * 11) >> 5, iy = xy - 3 * ix;
     const double X = __dsub_rn(img_coord(r.x, P.L[0], ix), cx);
     const double Y = __dsub_rn(img_coord(r.y, P.L[1], iy), cy);
+    const double XY2 = fma(X, X, Y * Y);
+    double c3 = 0, c5 = 0;
 #pragma unroll
     for (int iz = 0; iz < 3; ++iz) {
       if (!((bits >> iz) & 1u)) continue;
-      const d3 v = expansion64(g, mm, mk3(X, Y, Rz[iz]));
-      if (3 * xy + iz == kPrimary) nl = nl + v; else im = im + v;
+      const double Z = Rz[iz];
+      const double inv = rsqrt(fma(Z, Z, XY2));
+      const double inv2 = inv * inv;
+      const double i3 = inv2 * inv;
+      const double i5 = (i3 * inv2) * Z;
+      c3 += i3;
+      c5 += i5;
+      pz = fma(i3, Z, pz);
+      qz = fma(i5, Z, qz);
     }
+    px = fma(c3, X, px);
+    py = fma(c3, Y, py);
+    qx = fma(c5, X, qx);
+    qy = fma(c5, Y, qy);
+    sv += c3;
   }
+  // g x P + m x Q + (m21 S, 0, 0), m = (m02, m12, m22)
+  const double m21 = mm[0], m02 = mm[1], m12 = mm[2], m22 = mm[3];
+  im = im + mk3(fma(g[1], pz, fma(-g[2], py, fma(m12, qz, fma(-m22, qy, m21 * sv)))),
+                fma(g[2], px, fma(-g[0], pz, fma(m22, qx, -m02 * qz))),
+                fma(g[0], py, fma(-g[1], px, fma(m02, qy, -m12 * qx))));
 }
 
 // resident blocks per SM the register allocation must allow, measured at
@@ -649,8 +678,9 @@ __device__ __forceinline__ void cell_fp64(const OvParams& P, const Cell* cp, dou
 //   mixed 47.6 / 40.6 / 43.8 / 44.8 for 3 / 4 / 5 / 6 blocks (136 and 128
 //   registers without spills, 96 registers and 56 bytes spilled, 80
 //   registers and 272 bytes spilled)
-//   FP64 93.4 / 84.7 / 81.0 for 4 / 5 / 6 blocks (102 and 96 registers
-//   without spills, 80 registers and 84 bytes spilled)
+//   FP64 87.6 / 79.8 / 78.5 for 4 / 5 / 6 blocks (110 registers without
+//   spills, 96 registers and 48 bytes spilled, 80 registers and 88 bytes
+//   spilled)
 #ifndef OV_WALK_MULTI_MIN_BLOCKS_MIXED
 #define OV_WALK_MULTI_MIN_BLOCKS_MIXED 4
 #endif
