@@ -236,6 +236,7 @@ constexpr int kMultiWarps = 4;
 // (half a box less a rounding allowance; DBL_MAX on axes without shifts).
 struct ImageShortcut {
   double hw[3];
+  double half[3];   // L / 2 on periodic axes (the reference's wrap test), DBL_MAX otherwise
   int on;
 };
 
@@ -251,21 +252,6 @@ __device__ __forceinline__ double wrapped_sq(const OvParams& P, int a, double v,
   return __dmul_rn(u, u);
 }
 
-// the same with the unwrapped difference c - v in d (every axis)
-__device__ __forceinline__ double wrapped_sq_d(const OvParams& P, int a, double v, double c, double& d) {
-  double cc = c;
-  d = __dsub_rn(c, v);
-  if (P.periodic[a]) {
-    if (d > P.L[a] * 0.5) cc = __dsub_rn(c, P.L[a]);
-    else if (d < -P.L[a] * 0.5) cc = __dadd_rn(c, P.L[a]);
-  }
-  double u = __dsub_rn(v, cc);
-  return __dmul_rn(u, u);
-}
-
-__device__ __forceinline__ double sel3(int i, double a, double b, double c) {
-  return i == 0 ? a : (i == 1 ? b : c);
-}
 __device__ __forceinline__ float sel3f(int i, float a, float b, float c) {
   return i == 0 ? a : (i == 1 ? b : c);
 }
@@ -754,9 +740,15 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
         // fails.  Otherwise (and at the root, whose centre of mass may lie
         // outside the box) all decisions are taken in full.
         unsigned pass;
-        double dx, dy, dz;
-        const double q0 = __dadd_rn(__dadd_rn(wrapped_sq_d(P, 0, r.x, cx, dx), wrapped_sq_d(P, 1, r.y, cy, dy)),
-                                    wrapped_sq_d(P, 2, r.z, cz, dz));
+        // The reference wraps an axis when c - r lies outside [-L/2, L/2];
+        // where no axis wraps its squared distance is that of c - r itself
+        // (fl(r - c) = -fl(c - r)), bit for bit.
+        const double dx = __dsub_rn(cx, r.x), dy = __dsub_rn(cy, r.y), dz = __dsub_rn(cz, r.z);
+        double q0;
+        if (fabs(dx) <= S.half[0] && fabs(dy) <= S.half[1] && fabs(dz) <= S.half[2])
+          q0 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+        else
+          q0 = __dadd_rn(__dadd_rn(wrapped_sq(P, 0, r.x, cx), wrapped_sq(P, 1, r.y, cy)), wrapped_sq(P, 2, r.z, cz));
         const double E = (double)__int_as_float(h.y);
         const bool shortcut = sane && q > 0;
         if (shortcut && q0 >= t0.x + E) {
@@ -999,6 +991,7 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
       }
       if (shifted && !P.periodic[a]) sc.on = 0;
       sc.hw[a] = shifted ? 0.5 * P.L[a] - allowance : DBL_MAX;
+      sc.half[a] = P.periodic[a] ? P.L[a] * 0.5 : DBL_MAX;
     }
   }
   cudaEventRecord(s->ev1, s->stream);
