@@ -445,9 +445,11 @@ constexpr int kColumnImages = 8;
 // moments at R = r - L s - com formed in FP64 and rounded once, summed in
 // factored form and added to nl; images within the near radius in FP64
 // (expansion64_at, added to nl as they come).  m21 is the FP32 m21 moment
-// (the cell header's first word), thr the cell's opening threshold.
+// (the cell header's first word), thr the cell's opening threshold, dc the
+// opening test's FP64 difference com - r.
 __device__ __forceinline__ void cell_mixed(const OvParams& P, const Cell* cp, float m21, double cx, double cy,
-                                           double cz, double thr, d3 r, unsigned pass, double near2, d3& nl) {
+                                           double cz, double thr, d3 r, d3 dc, unsigned pass, double near2,
+                                           d3& nl) {
   const float2 q0f = *reinterpret_cast<const float2*>(&cp->f_g[0]);
   const float2 q1f = *reinterpret_cast<const float2*>(&cp->f_g[2]);
   const float2 q2f = *reinterpret_cast<const float2*>(&cp->f_m12);
@@ -456,13 +458,13 @@ __device__ __forceinline__ void cell_mixed(const OvParams& P, const Cell* cp, fl
   {
     // FP32 copies of the FP64-formed offsets r - L s - com per axis and shift
     const float Fx[3] = {(float)__dsub_rn(img_coord(r.x, P.L[0], 0), cx),
-                         (float)__dsub_rn(r.x, cx),
+                         -(float)dc.x,
                          (float)__dsub_rn(img_coord(r.x, P.L[0], 2), cx)};
     const float Fy[3] = {(float)__dsub_rn(img_coord(r.y, P.L[1], 0), cy),
-                         (float)__dsub_rn(r.y, cy),
+                         -(float)dc.y,
                          (float)__dsub_rn(img_coord(r.y, P.L[1], 2), cy)};
     const float Fz[3] = {(float)__dsub_rn(img_coord(r.z, P.L[2], 0), cz),
-                         (float)__dsub_rn(r.z, cz),
+                         -(float)dc.z,
                          (float)__dsub_rn(img_coord(r.z, P.L[2], 2), cz)};
     // an accepting image has |R|^2 >= its wrapped squared distance >=
     // thr, so a cell whose thr reaches the near radius needs no test
@@ -784,7 +786,7 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
           n_far += __popc(pass);
           // expansion at every accepting image: R = r - L s - com, unwrapped
           if (kMixed) {
-            cell_mixed(P, cp, __int_as_float(h.x), cx, cy, cz, t0.x, r, pass, near2, nl);
+            cell_mixed(P, cp, __int_as_float(h.x), cx, cy, cz, t0.x, r, mk3(dx, dy, dz), pass, near2, nl);
           } else {
             cell_fp64(P, cp, cx, cy, cz, r, pass, nl, im);
           }
