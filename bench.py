@@ -680,8 +680,34 @@ def bench_reconnect(args, ov, tangle, p):
     t0 = _t.perf_counter()
     nrec = lib.ov_reconnect_vortices(hc.ptr(), 0.0, rec_dist, rec_angle)
     t_pass = _t.perf_counter() - t0
+    from openvort_b200._lib import ReconnectStats
+    st = ReconnectStats()
+    lib.ov_reconnect_get_stats(C.byref(st))
     out = {"workload": f"{int(tangle.active.sum())} points, rec_dist={rec_dist}, rec_angle={rec_angle}",
-           "candidates": ncand, "reconnections": nrec, "gpu_search_s": t_search, "gpu_pass_s": t_pass}
+           "candidates": ncand, "reconnections": nrec, "gpu_search_s": t_search, "gpu_pass_s": t_pass,
+           "tested": st.tested, "nodes_summed": st.nodes_summed, "sums_s": st.sums_s,
+           "upload_and_search_s": st.search_s}
+    # mixed form: FP32 far-field sums with an error bound per node, FP64
+    # again where the bound leaves the approach test's sign open
+    ov.configure(p, ov.OV_PREC_MIXED)
+    hm = ht.copy()
+    hm.set_images_from_library(lib)
+    hm.recalc[:] = 0
+    t0 = _t.perf_counter()
+    nrec_m = lib.ov_reconnect_vortices(hm.ptr(), 0.0, rec_dist, rec_angle)
+    t_mixed = _t.perf_counter() - t0
+    ov.configure(p, ov.OV_PREC_FP64)
+    st = ReconnectStats()
+    lib.ov_reconnect_get_stats(C.byref(st))
+    act = hc.active
+    dv = np.linalg.norm(hm.vels[act] - hc.vels[act], axis=1) / np.maximum(np.linalg.norm(hc.vels[act], axis=1),
+                                                                           1e-300)
+    out["mixed"] = {"gpu_pass_s": t_mixed, "reconnections": nrec_m, "tested": st.tested,
+                    "nodes_summed": st.nodes_summed, "fp64_rechecks": st.fp64_rechecks, "sums_s": st.sums_s,
+                    "upload_and_search_s": st.search_s,
+                    "same_links_as_fp64": bool(np.array_equal(hm.links, hc.links) and nrec_m == nrec),
+                    "max_rel_err_vels_vs_fp64": float(dv.max()) if dv.size else 0.0,
+                    "speedup_over_fp64_pass": t_pass / t_mixed if t_mixed > 0 else None}
     from oracle.oracle import Ref, have_ref
     if have_ref():
         small, _ = make_tangle(20000, args.seed + 7)

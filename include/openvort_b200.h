@@ -474,6 +474,24 @@ int ov_reconnect_candidates(const struct tangle_state *tangle, double rec_dist, 
                             int *pairs, int max_pairs);
 int ov_reconnect_vortices(struct tangle_state *tangle, double t, double rec_dist, double rec_angle);
 
+/* In the mixed form (ov_set_precision(OV_PREC_MIXED)) ov_reconnect_vortices
+ * takes the approach test's Biot-Savart sums with the FP32 far field and a
+ * bound on their error per node; a test whose sign that bound leaves open
+ * is taken again with FP64 sums, so links, flags and count are the FP64
+ * form's, and the velocities it writes carry the mixed form's error.
+ * Counters of the last ov_reconnect_vortices call on this thread: */
+typedef struct {
+  int candidates;     /* pairs that passed the static tests */
+  int tested;         /* approach tests taken */
+  int nodes_summed;   /* nodes whose sums came from a batched direct sum */
+  int fp64_rechecks;  /* mixed form: tests taken again with FP64 sums */
+  int reconnections;
+  double search_s;    /* host seconds: upload and the GPU pair search */
+  double sums_s;      /* host seconds in the batched (and re-check) sums */
+  double total_s;     /* host seconds of the whole call */
+} ov_reconnect_stats;
+int ov_reconnect_get_stats(ov_reconnect_stats *out);
+
 /* ----- remesh and periodic wrap-around -----
  * ov_remesh replaces remesh (src/tangle.c:824-873, include/tangle.h:155):
  * the reference's slot-order loop that removes a node when a segment next

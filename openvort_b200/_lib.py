@@ -36,7 +36,7 @@ FUNCTIONS = [
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
     "ov_adjoint_velocity_vjp", "ov_adjoint_forward", "ov_adjoint_backward", "ov_adjoint_generation",
-    "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_remesh", "ov_enforce_boundaries", "ov_eliminate_small_loops",
+    "ov_reconnect_candidates", "ov_reconnect_vortices", "ov_reconnect_get_stats", "ov_remesh", "ov_enforce_boundaries", "ov_eliminate_small_loops",
     "ov_save_tangle", "ov_save_frame", "ov_state_save_frame", "ov_frame_wait", "ov_frame_info",
     "ov_load_frame", "ov_check_fast_math",
 ]
@@ -75,6 +75,12 @@ class RunStats(C.Structure):
 class BatchTuning(C.Structure):
     _fields_ = [("targets_per_block", C.c_int), ("sources_per_tile", C.c_int),
                 ("blocks_per_sm", C.c_int), ("kernel_ms", C.c_double)]
+
+
+class ReconnectStats(C.Structure):
+    _fields_ = ([(n, C.c_int) for n in ("candidates", "tested", "nodes_summed", "fp64_rechecks",
+                                        "reconnections")]
+                + [(n, C.c_double) for n in ("search_s", "sums_s", "total_s")])
 
 
 class BatchStats(C.Structure):
@@ -161,6 +167,7 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_adjoint_generation": (C.c_ulonglong, [C.c_void_p]),
         "ov_reconnect_candidates": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p, C.c_int]),
         "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
+        "ov_reconnect_get_stats": (C.c_int, [C.POINTER(ReconnectStats)]),
         "ov_remesh": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p]),
         "ov_enforce_boundaries": (C.c_int, [T]),
         "ov_eliminate_small_loops": (C.c_int, [T, C.c_int]),

@@ -123,7 +123,10 @@ constexpr int kPTgt = kPB * kTT;    // targets per block
 constexpr int kPSrc = 128;          // sources per shared-memory tile (kPSrc / 2 records)
 // interactions (targets x segments x (1 + images)) up to which the mixed
 // direct sum runs in slot order without the key sort
-constexpr double kSlotOrderWork = 2e8;
+#ifndef OV_SLOT_ORDER_WORK
+#define OV_SLOT_ORDER_WORK 2e8
+#endif
+constexpr double kSlotOrderWork = OV_SLOT_ORDER_WORK;
 
 #ifndef OV_DIRECT_PAIRS_MIN_BLOCKS
 #define OV_DIRECT_PAIRS_MIN_BLOCKS 5
@@ -387,6 +390,132 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_CHAIN_MIN_BLOCKS) k_direct_mixe
   }
 }
 
+// Mixed form at explicit points, with a bound on its rounding error.  The
+// reconnection pass (src/vortex_dynamics.c:266-281) needs only the sign of
+// its approach test from these sums, so each point also gets
+//   E = kMixedBoundU * kappa/4pi * sum |d| / |R|^2
+// over the pairs evaluated in FP32 (all others take the FP64 formula, and
+// the colinear ones are zero in both), which bounds |mixed - FP64| of the
+// tangle's own sum plus its image sum.  Per FP32 pair, with u = 2^-24, a
+// far pair (|R| >= 4 |d|) and |v| <= 1.6 kappa/4pi |d| / |R|^2:
+//   - inputs: the two-float R carries <= 4u |R|, d <= 2u |d|; the formula's
+//     sensitivity turns these into <= 28u kappa/4pi |d| / |R|^2;
+//   - evaluation: ~20 FP32 roundings plus rsqrt.approx (2^-22.9) and
+//     rcp.approx (1 ulp), the cross product's absolute error <= 2u |R||d|
+//     per component: <= 25u kappa/4pi |d| / |R|^2;
+//   - the FP32 partial sums of 16 terms per half: <= 26u of the sum of
+//     |v| over those terms.
+// Together <= 79u; kMixedBoundU = 256u leaves a factor of three.
+// Targets: explicit points, two-float offsets from the coordinate origin
+// (so a batch of points anywhere in the box keeps R to a few ulps of |R|),
+// skip[i] the slot whose own segments the tangle's sum leaves out.
+constexpr double kMixedBoundU = 256.0 / 16777216.0;
+
+__global__ void __launch_bounds__(kPB) k_direct_mixed_points(OvParams P, SegTab S, int n_src,
+                                                             const double* __restrict__ pos,
+                                                             const double* __restrict__ tpos,
+                                                             const int* __restrict__ tskip, int n_t,
+                                                             double* __restrict__ part,
+                                                             double* __restrict__ bpart, int chunk) {
+  __shared__ PairSrc<true> sh[kPSrc / 2];
+  const int j = blockIdx.y;   // 0: the tangle itself, j >= 1: image j-1
+  const int base = blockIdx.x * kPTgt;
+  bool act[kTT];
+  int kk[kTT];
+  d3 rr[kTT];
+  PairTargets T;
+#pragma unroll
+  for (int u = 0; u < kTT; ++u) {
+    const int i = base + threadIdx.x + kPB * u;
+    act[u] = i < n_t;
+    d3 r = act[u] ? ld3(tpos, i) : mk3(0, 0, 0);
+    if (act[u] && j > 0) r = image_point(P, j - 1, r);
+    rr[u] = r;
+    kk[u] = act[u] && j == 0 && tskip ? tskip[i] : -1;
+    set_target(T, u, r.x, r.y, r.z);
+  }
+  double acc[kTT][3], eacc[kTT];
+#pragma unroll
+  for (int u = 0; u < kTT; ++u) acc[u][0] = acc[u][1] = acc[u][2] = eacc[u] = 0;
+  const double f4pi = P.f4pi;
+  // FP64 evaluation of segment id at target u, with the skip rule of
+  // calculate_vs_shift (src/tangle.c:567-569) for the tangle itself
+  auto special = [&](int u, int id) {
+#pragma unroll
+    for (int v = 0; v < kTT; ++v) {
+      if (v != u) continue;
+      if (!act[v] || id < 0) return;
+      const int fw = S.fwd[id];
+      if (j == 0 && (id == kk[v] || fw == kk[v])) return;
+      const double* sg = S.r1r2 + 6 * (size_t)id;
+      const d3 vv = seg_vel64(f4pi, mk3(sg[0], sg[1], sg[2]), mk3(sg[3], sg[4], sg[5]), rr[v]);
+      acc[v][0] += vv.x;
+      acc[v][1] += vv.y;
+      acc[v][2] += vv.z;
+    }
+  };
+  const int s_lo = blockIdx.z * chunk, s_hi = min(n_src, s_lo + chunk);
+  // sources in slot order; the tangle's own segments wrapped across a
+  // periodic face go to FP64, where the skip rule applies
+  auto stage_one = [&](int m) -> SrcVals {
+    const int fw = m < s_hi ? S.fwd[m] : -1;
+    if (fw < 0) return src_none();
+    const double* sg = S.r1r2 + 6 * (size_t)m;
+    const double dxx = sg[3] - sg[0], dyy = sg[4] - sg[1], dzz = sg[5] - sg[2];
+    double far2 = fmax(16.0 * (dxx * dxx + dyy * dyy + dzz * dzz), P.near2);
+    if (j == 0) {
+      const d3 e = ld3(pos, fw);
+      if (e.x != sg[3] || e.y != sg[4] || e.z != sg[5]) far2 = 1e30;
+    }
+    return src_from(sg[0], sg[1], sg[2], dxx, dyy, dzz, far2, m);
+  };
+  for (int sb = s_lo; sb < s_hi; sb += kPSrc) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < kPSrc / 2; q += kPB)
+      stage_pair(sh[q], stage_one(sb + 2 * q), stage_one(sb + 2 * q + 1));
+    __syncthreads();
+    for (int q0 = 0; q0 < kPSrc / 2; q0 += 16) {
+      f2 b[kTT][3], eb[kTT];
+#pragma unroll
+      for (int k = 0; k < kTT; ++k) b[k][0] = b[k][1] = b[k][2] = eb[k] = f2_splat(0.f);
+#pragma unroll 2
+      for (int q = q0; q < q0 + 16; ++q) pair_interact_impl<true, true>(sh[q], T, b, special, eb);
+#pragma unroll
+      for (int k = 0; k < kTT; ++k) {
+        float lo, hi;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          f2_unpack(b[k][c], lo, hi);
+          acc[k][c] += f4pi * ((double)lo + (double)hi);
+        }
+        f2_unpack(eb[k], lo, hi);
+        eacc[k] += (double)lo + (double)hi;
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kTT; ++u) {
+    const int i = base + threadIdx.x + kPB * u;
+    if (i >= n_t) continue;
+    const size_t slab = (size_t)blockIdx.z * gridDim.y + j;
+    double* o = part + slab * 3 * (size_t)n_t + 3 * (size_t)i;
+    o[0] = acc[u][0];
+    o[1] = acc[u][1];
+    o[2] = acc[u][2];
+    bpart[slab * (size_t)n_t + i] = eacc[u];
+  }
+}
+
+// bound[i] = kMixedBoundU * kappa/4pi * (sum over splits and images of bpart)
+__global__ void k_reduce_bounds(double f4pi, const double* __restrict__ bpart, int n_t, int slabs,
+                                double* bound) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_t) return;
+  double e = 0;
+  for (int z = 0; z < slabs; ++z) e += bpart[(size_t)z * n_t + i];
+  bound[i] = kMixedBoundU * f4pi * e;
+}
+
 // v_nl = part[0]; v_img = sum_j part[j] in image order (src/tangle.c:627-638);
 // mirror images reflect their velocity (src/tangle.c:633-634).  With source
 // splits, each image's partial sums are added split by split, in order.
@@ -431,17 +560,19 @@ static bool ensure_segtab(ov_state_impl* s, const double* pos) {
 }
 
 // Source splits for a grid of `blocks` target blocks: enough that a small
-// tangle still fills the GPU (about 4 blocks per SM), each split a whole
-// number of tiles of `tile` sources; returns the sources per split.
-static int source_chunk(int n_src, long long blocks, int tile, int* splits) {
+// tangle still fills the GPU (about `per_sm` blocks per SM, at most
+// `max_splits` splits), each split a whole number of tiles of `tile`
+// sources; returns the sources per split.
+static int source_chunk(int n_src, long long blocks, int tile, int* splits, int per_sm = 4,
+                        int max_splits = 16) {
   static int sms = 0;
   if (!sms) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 1;
   }
-  long long want = (4LL * sms + blocks - 1) / std::max(1LL, blocks);
-  int sp = (int)std::min<long long>(16, std::max<long long>(1, want));
+  long long want = ((long long)per_sm * sms + blocks - 1) / std::max(1LL, blocks);
+  int sp = (int)std::min<long long>(max_splits, std::max<long long>(1, want));
   int chunk = (n_src + sp - 1) / sp;
   chunk = std::max(tile, (chunk + tile - 1) / tile * tile);
   *splits = std::max(1, (n_src + chunk - 1) / chunk);
@@ -518,10 +649,11 @@ bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const doubl
   int nimg = out_img ? s->P.n_img : 0;
   SegTab S{s->seg64.as<double>(), s->segid.as<int>()};
   int n_src = only ? n_only : s->n;
-  // few points over many sources: split the sources so the GPU fills
+  // few points over many sources: split the sources so the GPU fills, about
+  // four waves of the kernel's 7 resident blocks per SM
   const int bx = (npts + kTB - 1) / kTB;
   int splits = 1;
-  const int chunk = source_chunk(std::max(1, n_src), (long long)bx * (nimg + 1), kTS, &splits);
+  const int chunk = source_chunk(std::max(1, n_src), (long long)bx * (nimg + 1), kTS, &splits, 32, 64);
   size_t bytes = sizeof(double) * 3 * (size_t)npts * (nimg + 1) * splits;
   if (!s->img_part.reserve(bytes)) return false;
   dim3 grid(bx, nimg + 1, splits);
@@ -535,6 +667,34 @@ bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const doubl
   P.n_img = nimg;
   k_reduce_images<<<(npts + 255) / 256, 256, 0, s->stream>>>(P, s->img_part.as<double>(), npts,
                                                               out_nl, out_img, splits);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  return true;
+}
+
+bool ov_direct_points_bounded(ov_state_impl* s, const double* pos, int npts, const double* pts,
+                              const int* skip, double* out_nl, double* out_img, double* out_bound) {
+  if (npts <= 0) return true;
+  if (!ensure_segtab(s, pos)) return false;
+  const int nimg = s->P.n_img;
+  SegTab S{s->seg64.as<double>(), s->segid.as<int>()};
+  const int bx = (npts + kPTgt - 1) / kPTgt;
+  int splits = 1;
+  // a few thousand points: about eight waves of the kernel's 4 resident
+  // blocks per SM, so the last wave's tail is a small share
+  const int chunk = source_chunk(std::max(1, s->n), (long long)bx * (nimg + 1), kPSrc, &splits, 32, 64);
+  const size_t slabs = (size_t)(nimg + 1) * splits;
+  // per-image partial sums (3 per point) followed by the bound partials
+  if (!s->img_part.reserve(sizeof(double) * 4 * (size_t)npts * slabs)) return false;
+  double* part = s->img_part.as<double>();
+  double* bpart = part + 3 * (size_t)npts * slabs;
+  k_direct_mixed_points<<<dim3(bx, nimg + 1, splits), kPB, 0, s->stream>>>(s->P, S, s->n, pos, pts, skip, npts,
+                                                                          part, bpart, chunk);
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  k_reduce_images<<<(npts + 255) / 256, 256, 0, s->stream>>>(s->P, part, npts, out_nl, out_img, splits);
+  OV_LAUNCHED();
+  k_reduce_bounds<<<(npts + 255) / 256, 256, 0, s->stream>>>(s->P.f4pi, bpart, npts, (int)slabs, out_bound);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   return true;

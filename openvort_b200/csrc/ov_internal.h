@@ -174,6 +174,10 @@ bool ov_shard_unpack(ov_state_impl* s, const double* xbuf, size_t xcap);
 bool ov_tree_walk_points(ov_state_impl* s, OvTree* tree, int npts, const double* pts,
                          const int* skip, double theta, double* out_nl, double* out_img);
 
+// stable LSD radix sort of 64-bit keys with int values (ov_tree.cu); the
+// result ends in (ka, va), (kb, vb) are scratch of the same sizes
+bool ov_radix_sort_u64(uint64_t* ka, int* va, uint64_t* kb, int* vb, int n, DevBuf& hist, DevBuf& scan_part,
+                       cudaStream_t st);
 // direct sums for all nodes -> v_nl, v_img
 bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* v_img);
 // direct sums at arbitrary points (device arrays), sources = all segments or
@@ -182,6 +186,10 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
 bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const double* pts,
                       const int* skip, const int* only, int n_only, double* out_nl,
                       double* out_img);
+// mixed-form direct sums at points (tangle and images, every segment), with
+// out_bound[i] bounding |mixed - FP64| of out_nl + out_img at point i
+bool ov_direct_points_bounded(ov_state_impl* s, const double* pos, int npts, const double* pts,
+                              const int* skip, double* out_nl, double* out_img, double* out_bound);
 // direct point query on caller-provided scratch (see ov_direct.cu)
 bool ov_direct_points_scratch(cudaStream_t st, const OvParams& P, const double* pos,
                               const int2* links, const int2* status, int n, int npts,

@@ -92,7 +92,7 @@ constexpr float kColHi = 1e-8f * (1.0f + 2.5e-3f);
 // two staged sources (index 0 in the low halves, 1 in the high halves):
 //   q0 = (ax ay) pairs   q1 = (az dx)   q2 = (dy dz)   q3 = (-dx -dy)
 //   q4 = (-dz d2)   q5 = (far2, id) pairs
-//   q6 = (lo parts of ax ay)   q7 = (lo part of az, unused): two-float form
+//   q6 = (lo parts of ax ay)   q7 = (lo part of az, |d|): two-float form
 template <bool kTwo>
 struct __align__(16) PairSrc {
   float4 q[kTwo ? 8 : 6];
@@ -130,7 +130,7 @@ __device__ __forceinline__ void stage_pair(PairSrc<kTwo>& o, const SrcVals& s0, 
   o.q[5] = make_float4(s0.far2, s1.far2, __int_as_float(s0.id), __int_as_float(s1.id));
   if constexpr (kTwo) {
     o.q[6] = make_float4(s0.lx, s1.lx, s0.ly, s1.ly);
-    o.q[7] = make_float4(s0.lz, s1.lz, 0.f, 0.f);
+    o.q[7] = make_float4(s0.lz, s1.lz, sqrtf(d20), sqrtf(d21));
   }
 }
 
@@ -154,22 +154,26 @@ __device__ __forceinline__ void set_target(PairTargets& t, int k, double px, dou
 // kappa/4pi factor) into b[k] (low half: source 0, high half: source 1);
 // pairs needing FP64 call special(k, id).  The two-float form takes R as
 // (a_hi - t_hi) + (a_lo - t_lo), which carries ~2 ulps of |R| itself
-// however far source and target are from the origin.
-template <bool kTwo, class Special>
-__device__ __forceinline__ void pair_interact(const PairSrc<kTwo>& src, const PairTargets& T,
-                                              f2 (&b)[kTT][3], Special&& special) {
+// however far source and target are from the origin.  With kBound (two-
+// float form only) eb[k] also accumulates |d| / |R|^2 over the pairs
+// evaluated here in FP32, the quantity that bounds their rounding error.
+template <bool kTwo, bool kBound, class Special>
+__device__ __forceinline__ void pair_interact_impl(const PairSrc<kTwo>& src, const PairTargets& T,
+                                                   f2 (&b)[kTT][3], Special&& special, f2 (&eb)[kTT]) {
+  static_assert(kTwo || !kBound, "the error bound needs |d|, staged in the two-float form");
   const float4 q0 = src.q[0], q1 = src.q[1], q2 = src.q[2], q3 = src.q[3], q4 = src.q[4], q5 = src.q[5];
   const f2 ax = f2_pack(q0.x, q0.y), ay = f2_pack(q0.z, q0.w), az = f2_pack(q1.x, q1.y);
   const f2 dx = f2_pack(q1.z, q1.w), dy = f2_pack(q2.x, q2.y), dz = f2_pack(q2.z, q2.w);
   const f2 ndx = f2_pack(q3.x, q3.y), ndy = f2_pack(q3.z, q3.w), ndz = f2_pack(q4.x, q4.y);
   const f2 d2 = f2_pack(q4.z, q4.w);
   const f2 one = f2_splat(1.0f), two = f2_splat(2.0f);
-  f2 alx, aly, alz;
+  f2 alx, aly, alz, dn;
   if constexpr (kTwo) {
     const float4 q6 = src.q[6], q7 = src.q[7];
     alx = f2_pack(q6.x, q6.y);
     aly = f2_pack(q6.z, q6.w);
     alz = f2_pack(q7.x, q7.y);
+    dn = f2_pack(q7.z, q7.w);
   }
 #pragma unroll
   for (int k = 0; k < kTT; ++k) {
@@ -202,6 +206,11 @@ __device__ __forceinline__ void pair_interact(const PairSrc<kTwo>& src, const Pa
     b[k][0] = f2_fma(Cx, sk, b[k][0]);
     b[k][1] = f2_fma(Cy, sk, b[k][1]);
     b[k][2] = f2_fma(Cz, sk, b[k][2]);
+    if constexpr (kBound) {
+      float i0, i1;
+      f2_unpack(ia * ia, i0, i1);
+      eb[k] = f2_fma(dn, f2_pack(ok0 ? i0 : 0.f, ok1 ? i1 : 0.f), eb[k]);
+    }
     const bool sp0 = !ok0 && !(far0 && tc0 < kColLo);
     const bool sp1 = !ok1 && !(far1 && tc1 < kColLo);
     if (sp0 || sp1) {
@@ -209,6 +218,13 @@ __device__ __forceinline__ void pair_interact(const PairSrc<kTwo>& src, const Pa
       if (sp1) special(k, __float_as_int(q5.w));
     }
   }
+}
+
+template <bool kTwo, class Special>
+__device__ __forceinline__ void pair_interact(const PairSrc<kTwo>& src, const PairTargets& T,
+                                              f2 (&b)[kTT][3], Special&& special) {
+  f2 unused[kTT];
+  pair_interact_impl<kTwo, false>(src, T, b, special, unused);
 }
 
 // ----------------------------------------------------------------------
@@ -220,10 +236,9 @@ __device__ __forceinline__ void pair_interact(const PairSrc<kTwo>& src, const Pa
 //   u = 1/(ab), den = 1 + R.R' u = 1 + cos, w = u / den
 //   v = kappa/4pi (1/a + 1/b) w (R x d)
 // R x d, with the segment vector d staged on its own, keeps the FP32 error
-// of the cross product at a few ulps of |R||d|.  1 - cos is first estimated
-// as 2 - den, whose error is below 1e-6; only a warp with a pair under
-// 2e-6 forms the exact |R x d|^2 u w of the reference's cut-off test
-// (src/tangle.c:505-506).  That is 24 lane operations and 2 hardware
+// of the cross product at a few ulps of |R||d|.  The reference's cut-off
+// test (src/tangle.c:505-506) takes 1 - cos = |R x d|^2 u w, as in the
+// two-source form.  That is 28 lane operations and 2 hardware
 // approximations per interaction, against 31 and 3 for the two-source form
 // above.  Segments that do not chain (a loop's closing segment, a segment
 // wrapped across a periodic face) take the two-source form from a list.
@@ -297,7 +312,7 @@ template <bool kTwo, class Special>
 __device__ __forceinline__ void chain_sweep(const ChainNode<kTwo>* sh_node, const ChainSeg* sh_seg,
                                             const PairTargets& T, double (&acc)[kTT][3], double f4pi,
                                             Special&& special) {
-  const f2 one = f2_splat(1.0f), two = f2_splat(2.0f);
+  const f2 one = f2_splat(1.0f);
   // node 0 of the tile for each target
   f2 Rx[kTT], Ry[kTT], Rz[kTT], R2[kTT], ia[kTT];
   {
@@ -353,28 +368,19 @@ __device__ __forceinline__ void chain_sweep(const ChainNode<kTwo>* sh_node, cons
         const f2 den = f2_fma(e, uu, one);
         const f2 w = uu * f2_rcp(den);
         const f2 s = (ia[u] + ib) * w;
-        const f2 est = two - den;   // 1 - cos, error below 1e-6
-        float r20, r21, s0, s1, e0, e1;
+        // 1 - cos = |C|^2 u w for every pair: far segments of a large
+        // tangle subtend angles whose 1 - cos lies below any cheaper
+        // estimate's error, so a pre-test on 2 - den decides almost none
+        const f2 tc = f2_fma(Cz, Cz, f2_fma(Cy, Cy, Cx * Cx)) * (uu * w);
+        float r20, r21, s0, s1, tc0, tc1;
         f2_unpack(R2[u], r20, r21);
         f2_unpack(s, s0, s1);
-        f2_unpack(est, e0, e1);
-        bool far0 = r20 >= sg.far2.x && sg.id[0] >= 0, far1 = r21 >= sg.far2.y && sg.id[1] >= 0;
-        bool ok0 = far0 && e0 > 2e-6f, ok1 = far1 && e1 > 2e-6f;
-        bool sp0 = sg.id[0] >= 0 && !far0, sp1 = sg.id[1] >= 0 && !far1;
-        if (__any_sync(0xffffffffu, (far0 && !ok0) || (far1 && !ok1))) {
-          // near the colinearity cut-off: the exact 1 - cos = |C|^2 u w
-          const f2 tc = f2_fma(Cz, Cz, f2_fma(Cy, Cy, Cx * Cx)) * (uu * w);
-          float tc0, tc1;
-          f2_unpack(tc, tc0, tc1);
-          if (far0 && !ok0) {
-            ok0 = tc0 > kColHi;
-            sp0 = !ok0 && !(tc0 < kColLo);
-          }
-          if (far1 && !ok1) {
-            ok1 = tc1 > kColHi;
-            sp1 = !ok1 && !(tc1 < kColLo);
-          }
-        }
+        f2_unpack(tc, tc0, tc1);
+        const bool far0 = r20 >= sg.far2.x && sg.id[0] >= 0, far1 = r21 >= sg.far2.y && sg.id[1] >= 0;
+        const bool ok0 = far0 && tc0 > kColHi, ok1 = far1 && tc1 > kColHi;
+        // near pairs and pairs within the cut-off's rounding band: FP64
+        const bool sp0 = sg.id[0] >= 0 && !ok0 && !(far0 && tc0 < kColLo);
+        const bool sp1 = sg.id[1] >= 0 && !ok1 && !(far1 && tc1 < kColLo);
         const f2 sk = f2_pack(ok0 ? s0 : 0.f, ok1 ? s1 : 0.f);
         b[u][0] = f2_fma(Cx, sk, b[u][0]);
         b[u][1] = f2_fma(Cy, sk, b[u][1]);

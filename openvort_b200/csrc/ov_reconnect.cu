@@ -17,7 +17,8 @@
 // the approach test (update_velocity of both nodes, on the current links)
 // and do_reconnection.
 #include <algorithm>
-#include <cub/device/device_radix_sort.cuh>
+#include <chrono>
+#include <cstdlib>
 #include <vector>
 
 #include "ov_internal.h"
@@ -232,9 +233,17 @@ __global__ void k_rec_pack(const int* __restrict__ nodes, int count, int n, cons
 
 struct RecState {
   ov_state_impl s;
-  DevBuf keys, keys2, ids, ids2, pairs, count, tmp, skip, pack;
+  DevBuf keys, keys2, ids, ids2, pairs, count, hist, scan_part, skip, pack;
   DevBuf batch, pts, bnl, bimg, known;   // batched velocities
+  DevBuf bound, two;                     // mixed form: error bounds, FP64 re-checks
 };
+
+// counters of the last ov_reconnect_vortices call on this thread
+thread_local ov_reconnect_stats g_rec_stats;
+
+double secs_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
 
 RecState& rec_state() {
   static thread_local RecState r;
@@ -318,14 +327,10 @@ bool find_candidates(RecState& R, const tangle_state* t, double rec_dist, double
                                                      R.keys.as<unsigned long long>(), R.ids.as<int>(), n);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
-  size_t tmp_bytes = 0;
-  OV_TRY_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, R.keys.as<unsigned long long>(),
-                                              R.keys2.as<unsigned long long>(), R.ids.as<int>(),
-                                              R.ids2.as<int>(), n, 0, 64, s->stream));
-  if (!R.tmp.reserve(std::max<size_t>(tmp_bytes, 16))) return false;
-  OV_TRY_CUDA(cub::DeviceRadixSort::SortPairs(R.tmp.p, tmp_bytes, R.keys.as<unsigned long long>(),
-                                              R.keys2.as<unsigned long long>(), R.ids.as<int>(),
-                                              R.ids2.as<int>(), n, 0, 64, s->stream));
+  // the tree build's radix sort; the sorted keys and ids end in keys / ids
+  if (!ov_radix_sort_u64(R.keys.as<uint64_t>(), R.ids.as<int>(), R.keys2.as<uint64_t>(), R.ids2.as<int>(), n,
+                         R.hist, R.scan_part, s->stream))
+    return false;
   int cap = std::max(1024, n / 4);
   const double cos_angle = cos(rec_angle);
   for (int attempt = 0; attempt < 2; ++attempt) {
@@ -333,7 +338,7 @@ bool find_candidates(RecState& R, const tangle_state* t, double rec_dist, double
     OV_TRY_CUDA(cudaMemsetAsync(R.count.p, 0, sizeof(int), s->stream));
     k_rec_scan<<<(n + 127) / 128, 128, 0, s->stream>>>(
         s->P, g, s->pos.as<double>(), s->links.as<int2>(), s->status.as<int2>(), s->tan.as<double>(),
-        R.keys2.as<unsigned long long>(), R.ids2.as<int>(), n, rec_dist, cos_angle, R.pairs.as<int2>(), cap,
+        R.keys.as<unsigned long long>(), R.ids.as<int>(), n, rec_dist, cos_angle, R.pairs.as<int2>(), cap,
         R.count.as<int>());
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
@@ -378,6 +383,7 @@ struct RecVel {
   std::vector<int> known;        // slots with velocities on the device
   std::vector<int> pos_of;       // slot -> index in known, -1 if not known
   std::vector<double> hv;        // 6 per known node: vels, vs
+  std::vector<double> bound;     // per known node: bound on |mixed - FP64| of its sums (0: FP64)
   double time = 0;
 };
 
@@ -410,7 +416,35 @@ bool refresh_known(RecState& R, RecVel& V) {
 // Nonlocal and image sums of new nodes on the current links (one batched
 // FP64 direct sum), added to the known set; then every known node's
 // epilogue and host copy.
-bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes) {
+// Nonlocal and image sums of the m nodes at `batch` (a device list) on the
+// current links into v_nl, v_img: FP64, or (mixed) the FP32 far field with
+// a bound on its error per node copied into hb.
+bool sum_nodes(RecState& R, const int* batch, int m, bool mixed, double* hb) {
+  ov_state_impl* s = &R.s;
+  if (!R.pts.reserve(sizeof(double) * 3 * (size_t)m) || !R.skip.reserve(sizeof(int) * (size_t)m) ||
+      !R.bnl.reserve(sizeof(double) * 3 * (size_t)m) || !R.bimg.reserve(sizeof(double) * 3 * (size_t)m) ||
+      !R.bound.reserve(sizeof(double) * (size_t)m))
+    return false;
+  k_rec_points<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->n, s->pos.as<double>(), R.pts.as<double>(),
+                                                        R.skip.as<int>(), s->dflag.as<int>());
+  OV_LAUNCHED();
+  const bool ok = mixed ? ov_direct_points_bounded(s, s->pos.as<double>(), m, R.pts.as<double>(),
+                                                   R.skip.as<int>(), R.bnl.as<double>(), R.bimg.as<double>(),
+                                                   R.bound.as<double>())
+                        : ov_direct_points(s, s->pos.as<double>(), m, R.pts.as<double>(), R.skip.as<int>(),
+                                           nullptr, 0, R.bnl.as<double>(), R.bimg.as<double>());
+  if (!ok) return false;
+  k_rec_scatter<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->n, R.bnl.as<double>(), R.bimg.as<double>(),
+                                                         s->v_nl.as<double>(), s->v_img.as<double>(),
+                                                         s->dflag.as<int>());
+  OV_LAUNCHED();
+  OV_TRY_CUDA(cudaGetLastError());
+  if (mixed)
+    OV_TRY_CUDA(cudaMemcpyAsync(hb, R.bound.p, sizeof(double) * (size_t)m, cudaMemcpyDeviceToHost, s->stream));
+  return true;
+}
+
+bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes, bool mixed) {
   ov_state_impl* s = &R.s;
   const int m = (int)nodes.size();
   if (m == 0) return true;
@@ -420,27 +454,34 @@ bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes) {
     V.known.push_back(k);
   }
   const int cnt = (int)V.known.size();
-  if (!R.known.reserve(sizeof(int) * (size_t)cnt) || !R.pts.reserve(sizeof(double) * 3 * (size_t)m) ||
-      !R.skip.reserve(sizeof(int) * (size_t)m) || !R.bnl.reserve(sizeof(double) * 3 * (size_t)m) ||
-      !R.bimg.reserve(sizeof(double) * 3 * (size_t)m))
-    return false;
+  V.bound.resize(cnt, 0.0);
+  if (!R.known.reserve(sizeof(int) * (size_t)cnt)) return false;
   // the whole list: growing R.known reallocates it without its contents
   OV_TRY_CUDA(cudaMemcpyAsync(R.known.as<int>(), V.known.data(), sizeof(int) * (size_t)cnt,
                               cudaMemcpyHostToDevice, s->stream));
-  const int* batch = R.known.as<int>() + old;
-  if (!s->P.lia_only) {
-    k_rec_points<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->n, s->pos.as<double>(),
-                                                          R.pts.as<double>(), R.skip.as<int>(), s->dflag.as<int>());
-    OV_LAUNCHED();
-    if (!ov_direct_points(s, s->pos.as<double>(), m, R.pts.as<double>(), R.skip.as<int>(), nullptr, 0,
-                          R.bnl.as<double>(), R.bimg.as<double>()))
-      return false;
-    k_rec_scatter<<<(m + 255) / 256, 256, 0, s->stream>>>(batch, m, s->n, R.bnl.as<double>(),
-                                                           R.bimg.as<double>(), s->v_nl.as<double>(),
-                                                           s->v_img.as<double>(), s->dflag.as<int>());
-    OV_LAUNCHED();
-    OV_TRY_CUDA(cudaGetLastError());
-  }
+  const auto t0 = std::chrono::steady_clock::now();
+  if (!s->P.lia_only && !sum_nodes(R, R.known.as<int>() + old, m, mixed, V.bound.data() + old)) return false;
+  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  g_rec_stats.sums_s += secs_since(t0);
+  g_rec_stats.nodes_summed += m;
+  return refresh_known(R, V);
+}
+
+// Both nodes of a candidate again with FP64 sums on the current links (the
+// mixed sums left the approach test's sign open); the known set's other
+// nodes keep their values.
+bool recheck_fp64(RecState& R, RecVel& V, int k, int l) {
+  ov_state_impl* s = &R.s;
+  const int two[2] = {k, l};
+  if (!R.two.reserve(sizeof(int) * 2)) return false;
+  const auto t0 = std::chrono::steady_clock::now();
+  OV_TRY_CUDA(cudaMemcpyAsync(R.two.p, two, sizeof(two), cudaMemcpyHostToDevice, s->stream));
+  if (!s->P.lia_only && !sum_nodes(R, R.two.as<int>(), 2, false, nullptr)) return false;
+  OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
+  g_rec_stats.sums_s += secs_since(t0);
+  V.bound[V.pos_of[k]] = 0.0;
+  V.bound[V.pos_of[l]] = 0.0;
+  ++g_rec_stats.fp64_rechecks;
   return refresh_known(R, V);
 }
 
@@ -474,14 +515,37 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
   }
   RecState& R = rec_state();
   std::vector<int2> cand;
+  const auto t_start = std::chrono::steady_clock::now();
+  g_rec_stats = ov_reconnect_stats{};
   if (!upload_for_pass(R, tangle) || !find_candidates(R, tangle, rec_dist, rec_angle, cand))
     return -ov_last_error();
+  g_rec_stats.search_s = secs_since(t_start);
   ov_state_impl* s = &R.s;
   if (!ov_cuda_ok(cudaMemsetAsync(s->dflag.p, 0, sizeof(int), s->stream), "cudaMemsetAsync"))
     return -ov_last_error();
   RecVel V;
   V.pos_of.assign(tangle->N, -1);
   V.time = t;
+  g_rec_stats.candidates = (int)cand.size();
+  // Mixed form: the approach test's sums with the FP32 far field and a
+  // bound E on their error per node.  vels is affine in the sums (the
+  // epilogue, src/tangle.c:643-684, adds terms of the local velocity and of
+  // t' x (v_n - v_s) and t' x (t' x (v_n - v_s))), so vels moves by at most
+  // (1 + |alpha| |t'| + |alpha'| |t'|^2) E, and dx . dv by |dx| times the
+  // two nodes' sum of that.  A test whose |dx . dv| is within it (plus
+  // 1e-13 of |dx| (|v_k| + |v_l|) for the FP64 arithmetic) is taken again
+  // with FP64 sums, so every decision is the FP64 form's.
+  const bool mixed = s->P.precision == OV_PREC_MIXED;
+  // OV_RECONNECT_MARGIN_SCALE multiplies that margin (a huge value takes
+  // every mixed test again in FP64; for tests of this path)
+  double margin_scale = 1.0;
+  if (const char* e = getenv("OV_RECONNECT_MARGIN_SCALE")) margin_scale = atof(e);
+  auto amp = [&](int k) {
+    if (!s->P.use_mf) return 1.0;
+    const double* tk = tangle->tangents[k].p;
+    const double tn = sqrt(tk[0] * tk[0] + tk[1] * tk[1] + tk[2] * tk[2]);
+    return 1.0 + fabs(s->P.alpha) * tn + fabs(s->P.alpha_p) * tn * tn;
+  };
   // the nodes of this many upcoming candidates per batched direct sum
   constexpr int kBatchNodes = 2048;
   // recalculate holds the sit-out flags on entry: the reference zeroes them
@@ -509,27 +573,48 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
           }
       }
       for (int x : batch) V.pos_of[x] = -1;
-      if (!compute_nodes(R, V, batch)) return -ov_last_error();
+      if (!compute_nodes(R, V, batch, mixed)) return -ov_last_error();
+    }
+    ++g_rec_stats.tested;
+    // approach test (src/vortex_dynamics.c:266-281) on the known values
+    double w[3], dx[3];
+    h_pwrap(tangle, tangle->vnodes[k].p, tangle->vnodes[l].p, w);
+    for (int c = 0; c < 3; ++c) dx[c] = tangle->vnodes[k].p[c] - w[c];
+    auto approach = [&](double& dot, double& scale) {
+      const double* hk = V.hv.data() + 6 * (size_t)V.pos_of[k];
+      const double* hl = V.hv.data() + 6 * (size_t)V.pos_of[l];
+      dot = 0;
+      double vk2 = 0, vl2 = 0;
+      for (int c = 0; c < 3; ++c) {
+        dot += dx[c] * (hk[c] - hl[c]);
+        vk2 += hk[c] * hk[c];
+        vl2 += hl[c] * hl[c];
+      }
+      scale = sqrt(vk2) + sqrt(vl2);
+    };
+    double dot, vscale;
+    approach(dot, vscale);
+    if (mixed) {
+      const double ek = V.bound[V.pos_of[k]], el = V.bound[V.pos_of[l]];
+      const double dxn = sqrt(dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+      const double margin = margin_scale * dxn * (amp(k) * ek + amp(l) * el + 1e-13 * vscale);
+      if ((ek > 0 || el > 0) && !(fabs(dot) > margin)) {
+        if (!recheck_fp64(R, V, k, l)) return -ov_last_error();
+        approach(dot, vscale);
+      }
     }
     // update_velocity of both nodes writes their vels and vs (as the
     // reference's does, src/vortex_dynamics.c:275-276)
-    const double* hk = V.hv.data() + 6 * (size_t)V.pos_of[k];
-    const double* hl = V.hv.data() + 6 * (size_t)V.pos_of[l];
-    for (int c = 0; c < 3; ++c) {
-      tangle->vels[k].p[c] = hk[c];
-      tangle->vs[k].p[c] = hk[3 + c];
-      tangle->vels[l].p[c] = hl[c];
-      tangle->vs[l].p[c] = hl[3 + c];
+    {
+      const double* hk = V.hv.data() + 6 * (size_t)V.pos_of[k];
+      const double* hl = V.hv.data() + 6 * (size_t)V.pos_of[l];
+      for (int c = 0; c < 3; ++c) {
+        tangle->vels[k].p[c] = hk[c];
+        tangle->vs[k].p[c] = hk[3 + c];
+        tangle->vels[l].p[c] = hl[c];
+        tangle->vs[l].p[c] = hl[3 + c];
+      }
     }
-    // approach test (src/vortex_dynamics.c:266-281)
-    double w[3], dx[3], dv[3];
-    h_pwrap(tangle, tangle->vnodes[k].p, tangle->vnodes[l].p, w);
-    for (int c = 0; c < 3; ++c) {
-      dx[c] = tangle->vnodes[k].p[c] - w[c];
-      dv[c] = tangle->vels[k].p[c] - tangle->vels[l].p[c];
-    }
-    double dot = 0;
-    for (int c = 0; c < 3; ++c) dot += dx[c] * dv[c];
     if (dot > 0) continue;
     const int knext = tangle->connections[k].forward, kprev = tangle->connections[k].reverse;
     const int lnext = tangle->connections[l].forward, lprev = tangle->connections[l].reverse;
@@ -557,16 +642,21 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     // segment, whose local term is not finite)
     {
       std::vector<int> keep;
+      std::vector<double> keep_bound;
       keep.reserve(V.known.size());
-      for (int x : V.known) {
+      keep_bound.reserve(V.known.size());
+      for (size_t q = 0; q < V.known.size(); ++q) {
+        const int x = V.known[q];
         if (tangle->recalculate[x]) {
           V.pos_of[x] = -3;   // retired
         } else {
           V.pos_of[x] = (int)keep.size();
           keep.push_back(x);
+          keep_bound.push_back(V.bound[q]);
         }
       }
       V.known.swap(keep);
+      V.bound.swap(keep_bound);
       if (!V.known.empty() &&
           !ov_cuda_ok(cudaMemcpyAsync(R.known.as<int>(), V.known.data(), sizeof(int) * V.known.size(),
                                       cudaMemcpyHostToDevice, s->stream),
@@ -590,7 +680,18 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     if (!refresh_known(R, V)) return -ov_last_error();
   }
   if (!ov_cuda_ok(cudaStreamSynchronize(s->stream), "cudaStreamSynchronize")) return -ov_last_error();
+  g_rec_stats.reconnections = nrecs;
+  g_rec_stats.total_s = secs_since(t_start);
   return nrecs;
+}
+
+int ov_reconnect_get_stats(ov_reconnect_stats* out) {
+  if (!out) {
+    ov_set_error(OV_ERR_INVALID, "ov_reconnect_get_stats: null output");
+    return -OV_ERR_INVALID;
+  }
+  *out = g_rec_stats;
+  return 0;
 }
 
 }  // extern "C"

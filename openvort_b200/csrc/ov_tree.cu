@@ -25,6 +25,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <utility>
 
 #include "ov_internal.h"
 
@@ -796,6 +797,29 @@ static bool scan_excl(unsigned* v, int m, DevBuf& part, cudaStream_t st) {
   return ov_cuda_ok(cudaGetLastError(), "scan");
 }
 
+// Stable LSD radix sort of n 64-bit keys with int values, 8 passes of 8
+// bits (k_rs_hist, the three-launch scan, k_rs_scatter).  (kb, vb) are the
+// alternate buffers; after the even number of passes the sorted keys and
+// values are back in (ka, va).
+bool ov_radix_sort_u64(uint64_t* ka, int* va, uint64_t* kb, int* vb, int n, DevBuf& hist, DevBuf& scan_part,
+                       cudaStream_t st) {
+  if (n <= 0) return true;
+  const int nb = (n + kRsTile - 1) / kRsTile;
+  if (!hist.reserve(sizeof(unsigned) * 256 * (size_t)nb)) return false;
+  for (int pass = 0; pass < 8; ++pass) {
+    const int shift = 8 * pass;
+    k_rs_hist<<<nb, kRsThreads, 0, st>>>(ka, n, shift, hist.as<unsigned>(), nb);
+    OV_LAUNCHED();
+    if (!scan_excl(hist.as<unsigned>(), 256 * nb, scan_part, st)) return false;
+    k_rs_scatter<<<nb, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, hist.as<unsigned>(), nb);
+    OV_LAUNCHED();
+    OV_TRY_CUDA(cudaGetLastError());
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  return true;
+}
+
 bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
   const int n = s->n;
   cudaStream_t st = s->stream;
@@ -837,26 +861,13 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
   }
   const int na = hc[0];
   T->n_nodes = na;
-  // radix sort over the high word (8 passes of 8 bits), stable
-  uint64_t *ka = khi, *kb = khi_alt;
-  int *va = vals, *vb = vals_alt;
-  // vals_alt's second half holds the sorted term codes: sort into a separate
-  // scratch for values instead
+  // radix sort over the high word (8 passes of 8 bits), stable; vals_alt's
+  // second half holds the sorted term codes, so the values alternate with a
+  // separate scratch.  The sorted data ends back in khi / vals.
+  uint64_t* ka = khi;
+  int* va = vals;
   if (!T->scratch.reserve(sizeof(int) * (size_t)n + 16)) return false;
-  int* vtmp = T->scratch.as<int>();
-  vb = vtmp;
-  for (int pass = 0; pass < 8 && n > 0; ++pass) {
-    int shift = 8 * pass;
-    k_rs_hist<<<nb_rs, kRsThreads, 0, st>>>(ka, n, shift, T->hist.as<unsigned>(), nb_rs);
-    OV_LAUNCHED();
-    if (!scan_excl(T->hist.as<unsigned>(), 256 * nb_rs, T->scan_part, st)) return false;
-    k_rs_scatter<<<nb_rs, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, T->hist.as<unsigned>(), nb_rs);
-    OV_LAUNCHED();
-    OV_TRY_CUDA(cudaGetLastError());
-    uint64_t* tk = ka; ka = kb; kb = tk;
-    int* tv = va; va = vb; vb = tv;
-  }
-  // after an even number of passes the sorted data is back in khi / vals
+  if (!ov_radix_sort_u64(khi, vals, khi_alt, T->scratch.as<int>(), n, T->hist, T->scan_part, st)) return false;
   if (!T->perm.reserve(sizeof(int) * (size_t)(n > 0 ? n : 1))) return false;
   int* perm = T->perm.as<int>();
   if (n > 0) {

@@ -162,3 +162,79 @@ def test_sit_out_flags_are_read_on_entry(ov):
     assert ng == nw
     assert np.array_equal(out.links, want.links)
     assert not np.array_equal(out.links, base.links)
+
+
+def run_ours_mixed(ov, t, rec_dist, margin_scale=None):
+    """the pass in the mixed form: FP32 far field with an error bound per
+    node, FP64 sums again for tests whose sign the bound leaves open"""
+    import os
+    from openvort_b200._lib import ReconnectStats
+    lib = ov.load()
+    ov.configure(PARAMS, ov.OV_PREC_MIXED)
+    out = t.copy()
+    out.set_images_from_library(lib)
+    out.recalc[:] = 0
+    old = os.environ.get("OV_RECONNECT_MARGIN_SCALE")
+    if margin_scale is not None:
+        os.environ["OV_RECONNECT_MARGIN_SCALE"] = repr(margin_scale)
+    try:
+        n = lib.ov_reconnect_vortices(out.ptr(), 0.0, rec_dist, REC_ANGLE)
+    finally:
+        ov.configure(PARAMS, ov.OV_PREC_FP64)
+        if old is None:
+            os.environ.pop("OV_RECONNECT_MARGIN_SCALE", None)
+        else:
+            os.environ["OV_RECONNECT_MARGIN_SCALE"] = old
+    assert n >= 0, lib.ov_last_error_message()
+    st = ReconnectStats()
+    assert lib.ov_reconnect_get_stats(C.byref(st)) == 0
+    return out, n, st
+
+
+def dense_case(boundary):
+    ref = Ref()
+    D = 0.05
+    t = prepared(G.random_ring_tangle(17, 40, D, dl=D / 100, boundary=boundary), ref)
+    return ref, t, 2.5 * D / 100
+
+
+@pytest.mark.parametrize("boundary", ["open", "periodic-26"])
+def test_mixed_pass_takes_the_reference_decisions(ov, boundary):
+    """Mixed form: the same links, flags and count as the reference's FP64
+    pass; the velocities written at each test within the mixed form's 1e-5."""
+    ref, t, rec_dist = dense_case(boundary)
+    want, nw = ref.reconnect(t, PARAMS, 0.0, rec_dist, REC_ANGLE)
+    got, ng, st = run_ours_mixed(ov, t, rec_dist)
+    assert nw > 0
+    assert ng == nw == st.reconnections
+    assert np.array_equal(got.links, want.links)
+    assert np.array_equal(got.recalc, want.recalc)
+    assert st.tested > 0 and st.nodes_summed > 0
+    assert 0 <= st.fp64_rechecks <= st.tested
+    assert rel_err(got.vels, want.vels, t.active) < 1e-5
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_mixed_pass_crossing_rings(ov, seed):
+    ref = Ref()
+    t = prepared(crossing_rings(seed), ref)
+    rec_dist = 2 * 2 * np.pi * 1e-2 / 200
+    want, nw = ref.reconnect(t, PARAMS, 0.0, rec_dist, REC_ANGLE)
+    got, ng, st = run_ours_mixed(ov, t, rec_dist)
+    assert ng == nw
+    assert np.array_equal(got.links, want.links)
+    assert np.array_equal(got.recalc, want.recalc)
+    assert rel_err(got.vels, want.vels, t.active) < 1e-5
+
+
+def test_mixed_pass_fp64_rechecks(ov):
+    """A margin scaled beyond every |dx . dv| sends each test whose nodes
+    still carry mixed sums to the FP64 re-check: the decisions stay the
+    reference's and every velocity written is the FP64 one."""
+    ref, t, rec_dist = dense_case("periodic-26")
+    want, nw = ref.reconnect(t, PARAMS, 0.0, rec_dist, REC_ANGLE)
+    got, ng, st = run_ours_mixed(ov, t, rec_dist, margin_scale=1e300)
+    assert ng == nw
+    assert np.array_equal(got.links, want.links)
+    assert st.fp64_rechecks > 0
+    assert rel_err(got.vels, want.vels, t.active) < 1e-12
