@@ -935,6 +935,7 @@ def run_sharded(args, world, rank, local, dist):
                          "kernel": "Barnes-Hut walk, one rank's share of the targets (slowest rank)",
                          "peak_source": "ov_measure_fma_peak: FP32 FMA burst on this GPU, this run"},
             "independent_tangles": indep,
+            "process_group": D.describe(dist),
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,

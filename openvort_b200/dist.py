@@ -1,9 +1,11 @@
 """One process per GPU: the rank plumbing of multi-GPU runs.
 
-The hot path shards by independent tangles (each rank evolves its own
-seeded tangle, with no collective on the data path), so the only
-collectives are the timing ones: a barrier around the timed region and the
-maximum of the per-rank device times.  NCCL on GPUs, gloo on CPU (tests).
+Two multi-GPU forms use it: one tangle over all ranks (openvort_b200.shard,
+whose exchange is an all-gather of the Biot-Savart sums), and one
+independent tangle per rank (no collective on the data path).  Beyond that
+exchange the collectives are the timing ones: a barrier around the timed
+region and the maximum of the per-rank device times.  NCCL on GPUs, gloo on
+CPU (tests).
 """
 from __future__ import annotations
 
@@ -45,6 +47,19 @@ def setup(backend: str | None = None, timeout_s: float = 600.0) -> Ranks:
         device = f"cuda:{local}"
     dist.init_process_group(backend, **kw)
     return Ranks(world, rank, local, dist, device)
+
+
+def describe(r: Ranks) -> dict:
+    """The process group as the run saw it: backend, world size and, for
+    NCCL, the library version torch loaded."""
+    if r.pg is None:
+        return {"backend": None, "world": 1}
+    out = {"backend": r.pg.get_backend(), "world": r.pg.get_world_size()}
+    if out["backend"] == "nccl":
+        import torch
+        v = torch.cuda.nccl.version()
+        out["nccl_version"] = ".".join(map(str, v)) if isinstance(v, tuple) else str(v)
+    return out
 
 
 def rank_seed(seed: int, rank: int) -> int:

@@ -28,7 +28,7 @@ def _worker(rank, world, port, q, mode):
             D.barrier(r)
             mx = D.max_over_ranks(r, 1.5 + rank)
             sm = D.sum_over_ranks(r, 1.0 + rank)
-            q.put((rank, mx, sm, D.rank_seed(2024, rank)))
+            q.put((rank, mx, sm, D.rank_seed(2024, rank), D.describe(r)))
         elif mode == "exchange":
             # sharded evaluations: each rank's block of the exchange buffer,
             # all-gathered in place; the tail beyond world * block untouched
@@ -103,16 +103,18 @@ def test_single_process_needs_no_group(monkeypatch):
     r = D.setup()
     assert r.world == 1 and r.pg is None
     assert D.max_over_ranks(r, 3.0) == 3.0
+    assert D.describe(r) == {"backend": None, "world": 1}
     D.barrier(r)
 
 
 def test_timing_collectives_world_2():
     out = _run("collectives")
     assert [o[0] for o in out] == [0, 1]
-    for rank, mx, sm, seed in out:
+    for rank, mx, sm, seed, pg in out:
         assert mx == 2.5          # the slowest rank's time
         assert sm == 3.0
         assert seed == 2024 + 1000 * rank
+        assert pg == {"backend": "gloo", "world": 2}
     assert out[0][3] != out[1][3]  # every rank its own tangle
 
 
