@@ -233,7 +233,7 @@ __global__ void __launch_bounds__(kPB, OV_DIRECT_PAIRS_MIN_BLOCKS) k_direct_mixe
 // whatever a block's extent and no key sort is needed.  Measured: on a
 // 4096-point ring an RK4 step takes less than the FP64 form's (the key sort
 // of k_direct_mixed_pairs costs more than its sum there); on the 22.4k-point
-// periodic tangle k_direct_mixed_pairs is faster (18.6 against 27.1 ms).
+// periodic tangle k_direct_mixed_pairs is faster (18.6 against 24.4 ms).
 static_assert(2 * kCH == kPSrc, "a chain tile is the two-source form's tile");
 
 #ifndef OV_DIRECT_CHAIN_MIN_BLOCKS
