@@ -107,6 +107,132 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
   }
 }
 
+// FP64 in chain order: sources in slot order, where a loop's segments
+// follow one another (segment m runs from node m to its forward node m + 1
+// for all but one segment per loop).  Each node's R = r_node - r, |R|^2 and
+// refined 1/|R| are formed once per target and serve both segments that
+// touch it, so a chained segment costs its R.R', one refined reciprocal and
+// the cross product: about 42 FP64 operations against 55 for seg_vel64_nr.
+// R' is r2 - r itself, as the reference forms it (src/tangle.c:490-491).
+// The cut-offs are decided as in seg_vel64_nr: where |R| or |R'| is within
+// 1.5e-8 or cos within 2e-8 of 1, the reference's own operations decide
+// (seg_vel64).  Segments that do not chain (a loop's closing segment, one
+// wrapped across a periodic face) take seg_vel64_nr from a list.  Block =
+// kTB targets x one image; targets are node slots (status-filtered, skip =
+// the slot) or explicit points (kPoints, skip from tskip).
+constexpr int kCS = 128;   // chained segments per shared-memory tile
+static_assert(kCS == kTS, "the chain sweep splits sources as k_direct64 does");
+
+template <bool kPoints>
+__global__ void __launch_bounds__(kTB) k_direct64_chain(OvParams P, SegTab S, int n_src,
+                                                        const double* __restrict__ pos,
+                                                        const double* __restrict__ tpos,
+                                                        const int2* __restrict__ tstatus,
+                                                        const int* __restrict__ tskip, int n_t,
+                                                        double* __restrict__ part, int chunk) {
+  __shared__ double sh_node[kCS + 1][3];
+  __shared__ int sh_kind[kCS];   // 1: chained, 0: no segment or in the list
+  __shared__ int sh_irr[kCS];
+  __shared__ int sh_nirr;
+  const int j = blockIdx.y;   // 0: the tangle itself, j >= 1: image j-1
+  const int k = blockIdx.x * kTB + threadIdx.x;
+  bool act = k < n_t;
+  if (act && !kPoints) act = tstatus[k].x != OV_EMPTY && tstatus[k].x != OV_PINNED;
+  d3 r = mk3(0, 0, 0);
+  int skip = -1;
+  if (act) {
+    r = ld3(kPoints ? tpos : pos, k);
+    if (j > 0) r = image_point(P, j - 1, r);
+    else skip = kPoints ? (tskip ? tskip[k] : -1) : k;
+  }
+  double ax = 0, ay = 0, az = 0;
+  const double f4pi = P.f4pi;
+  const int s_lo = blockIdx.z * chunk, s_hi = min(n_src, s_lo + chunk);
+  for (int sb = s_lo; sb < s_hi; sb += kCS) {
+    __syncthreads();
+    if (threadIdx.x == 0) sh_nirr = 0;
+    __syncthreads();
+    // nodes sb .. sb + kCS (positions; a slot beyond the range or EMPTY is
+    // used by no chained segment)
+    for (int i = threadIdx.x; i <= kCS; i += kTB) {
+      const int m = sb + i;
+      const d3 p = m < n_src ? ld3(pos, m) : mk3(0, 0, 0);
+      sh_node[i][0] = p.x;
+      sh_node[i][1] = p.y;
+      sh_node[i][2] = p.z;
+    }
+    for (int i = threadIdx.x; i < kCS; i += kTB) {
+      const int m = sb + i;
+      const int fw = m < s_hi ? S.fwd[m] : -1;
+      int kind = 0;
+      if (fw >= 0) {
+        const double* sg = S.r1r2 + 6 * (size_t)m;
+        bool chained = fw == m + 1;
+        if (chained) {
+          const d3 e = ld3(pos, fw);
+          chained = e.x == sg[3] && e.y == sg[4] && e.z == sg[5];
+        }
+        if (chained) kind = 1;
+        else sh_irr[atomicAdd(&sh_nirr, 1)] = m;
+      }
+      sh_kind[i] = kind;
+    }
+    __syncthreads();
+    if (!act) continue;
+    // node 0 of the tile
+    d3 Ra = mk3(sh_node[0][0], sh_node[0][1], sh_node[0][2]) - r;
+    double Ra2 = dot3(Ra, Ra);
+    double ia = Ra2 >= 2.25e-16 ? rsqrt_nr(Ra2) : 0.0;
+    const int cnt = min(kCS, s_hi - sb);
+#pragma unroll 2
+    for (int i = 0; i < cnt; ++i) {
+      const d3 nb = mk3(sh_node[i + 1][0], sh_node[i + 1][1], sh_node[i + 1][2]);
+      const d3 Rb = nb - r;
+      const double Rb2 = dot3(Rb, Rb);
+      const double ib = Rb2 >= 2.25e-16 ? rsqrt_nr(Rb2) : 0.0;
+      const int m = sb + i;
+      // skip rule of calculate_vs_shift (src/tangle.c:567-569): segment m
+      // runs from m to m + 1
+      if (sh_kind[i] && m != skip && m + 1 != skip) {
+        d3 v;
+        const double RRp = dot3(Ra, Rb);
+        const double u = ia * ib;
+        if (Ra2 < 2.25e-16 || Rb2 < 2.25e-16 || fabs(fma(RRp, u, -1.0)) < 2e-8) {
+          v = seg_vel64(f4pi, mk3(sh_node[i][0], sh_node[i][1], sh_node[i][2]), nb, r);
+        } else {
+          const double sc = f4pi * (ia + ib) * (u * rcp_nr(fma(RRp, u, 1.0)));
+          v = cross3(Ra, Rb) * sc;
+        }
+        ax += v.x;
+        ay += v.y;
+        az += v.z;
+      }
+      Ra = Rb;
+      Ra2 = Rb2;
+      ia = ib;
+    }
+    // the segments that do not chain
+    const int nirr = sh_nirr;
+    for (int q = 0; q < nirr; ++q) {
+      const int m = sh_irr[q];
+      const int fw = S.fwd[m];
+      if (m == skip || fw == skip) continue;
+      const double* sg = S.r1r2 + 6 * (size_t)m;
+      const d3 r1 = mk3(sg[0], sg[1], sg[2]), r2 = mk3(sg[3], sg[4], sg[5]);
+      const d3 v = seg_vel64_nr(f4pi, r1, r2, r2 - r1, r);
+      ax += v.x;
+      ay += v.y;
+      az += v.z;
+    }
+  }
+  if (k < n_t) {
+    double* o = part + ((size_t)blockIdx.z * gridDim.y + j) * 3 * (size_t)n_t + 3 * (size_t)k;
+    o[0] = act ? ax : 0;
+    o[1] = act ? ay : 0;
+    o[2] = act ? az : 0;
+  }
+}
+
 // Mixed form, two sources per instruction.  Block = kPB threads x kTT
 // targets (the tree's key order, so close in space) x one image.  The
 // origin O is the block's first target, so a single rounding of the
@@ -624,11 +750,11 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
     // EMPTY slots are never read by the epilogue, but zero them for hygiene
   } else {
     const int bx = (s->n + kTB - 1) / kTB;
-    const int chunk = source_chunk(s->n, (long long)bx * (nimg + 1), kTS, &splits);
+    const int chunk = source_chunk(s->n, (long long)bx * (nimg + 1), kCS, &splits);
     if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;
     cudaEventRecord(s->ev1, s->stream);
-    k_direct64<<<dim3(bx, nimg + 1, splits), kTB, 0, s->stream>>>(
-        s->P, S, s->n, nullptr, pos, s->status.as<int2>(), nullptr, s->n, s->img_part.as<double>(), chunk);
+    k_direct64_chain<false><<<dim3(bx, nimg + 1, splits), kTB, 0, s->stream>>>(
+        s->P, S, s->n, pos, nullptr, s->status.as<int2>(), nullptr, s->n, s->img_part.as<double>(), chunk);
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
   }
@@ -657,8 +783,14 @@ bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const doubl
   size_t bytes = sizeof(double) * 3 * (size_t)npts * (nimg + 1) * splits;
   if (!s->img_part.reserve(bytes)) return false;
   dim3 grid(bx, nimg + 1, splits);
-  k_direct64<<<grid, kTB, 0, s->stream>>>(s->P, S, n_src, only, pts, nullptr, skip, npts,
-                                          s->img_part.as<double>(), chunk);
+  if (only) {
+    k_direct64<<<grid, kTB, 0, s->stream>>>(s->P, S, n_src, only, pts, nullptr, skip, npts,
+                                            s->img_part.as<double>(), chunk);
+  } else {
+    // all segments: the chain sweep over slot order (kCS == kTS: same splits)
+    k_direct64_chain<true><<<grid, kTB, 0, s->stream>>>(s->P, S, n_src, pos, pts, nullptr, skip, npts,
+                                                        s->img_part.as<double>(), chunk);
+  }
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
   // out_nl = part[0]; out_img = image sum in table order (src/tangle.c:624-638),
