@@ -589,9 +589,12 @@ def bench_adjoint(args, ov):
     d = rng.normal(size=(n, 3)) * dl
     eps = 1e-5
 
-    def lval(x0, vn):
-        xf = a.forward(x0, vn, 0.0, dt, steps, every)
+    def lval_of(adj, x0, vn):
+        xf = adj.forward(x0, vn, 0.0, dt, steps, every)
         return float(centroid_length_loss(torch.from_numpy(xf), fwd, t.active, target))
+
+    def lval(x0, vn):
+        return lval_of(a, x0, vn)
     fd = (lval(t.pos + eps * d, vn0) - lval(t.pos - eps * d, vn0)) / (2 * eps)
     e = np.array([1e-3, 0.0, 0.0])
     fdv = (lval(t.pos, vn0 + e) - lval(t.pos, vn0 - e)) / 2e-3
@@ -637,6 +640,21 @@ def bench_adjoint(args, ov):
     smooth_pos = abs(float(np.sum(x0t.grad.numpy() * d)) - fd2) / abs(fd2)
     smooth_vns = abs(float(vnt.grad.numpy()[0]) - fd2v) / abs(fd2v)
     a2.close()
+    # Trajectory-level check of config 5 as specified (sigma = 1e-4 cm) with
+    # the colinearity cut-off switched off in the FP64 sums and the adjoint
+    # (ov_set_colinear_cutoff(0)): the dynamics are then smooth, and the
+    # adjoint and the finite differences differentiate the same function
+    lib = ov.load()
+    lib.ov_set_colinear_cutoff(0.0)
+    try:
+        a3, gx3, gv3, _, _ = grads(ov.OV_PREC_FP64)
+        fd3 = (lval_of(a3, t.pos + eps * d, vn0) - lval_of(a3, t.pos - eps * d, vn0)) / (2 * eps)
+        fd3v = (lval_of(a3, t.pos, vn0 + e) - lval_of(a3, t.pos, vn0 - e)) / 2e-3
+        a3.close()
+    finally:
+        lib.ov_set_colinear_cutoff(1e-8)
+    nocut_pos = abs(float(np.sum(gx3 * d)) - fd3) / abs(fd3)
+    nocut_vns = abs(gv3[0] - fd3v) / abs(fd3v)
     am, gxm, gvm, tfm, tbm = grads(ov.OV_PREC_MIXED)
     am.close()
     ov.configure(p, ov.OV_PREC_FP64)
@@ -649,8 +667,10 @@ def bench_adjoint(args, ov):
             "mixed_fd_rel_err_vns": abs(gvm[0] - fdv) / abs(fdv),
             "velocity_vjp_fd_rel_err_masked": vel_masked, "discontinuous_nodes": int(bad.sum()),
             "fd_rel_err_positions_small_waves": smooth_pos, "fd_rel_err_vns_small_waves": smooth_vns,
+            "fd_rel_err_positions_no_colinear_cutoff": nocut_pos, "fd_rel_err_vns_no_colinear_cutoff": nocut_vns,
             "note": "fd_rel_err_* at 4096 points include the jumps of the reference's colinearity "
-                    "cut-off crossed between the perturbed runs"}
+                    "cut-off crossed between the perturbed runs; *_no_colinear_cutoff: the same input, "
+                    "FP64, with that cut-off switched off in the sums and the adjoint"}
 
 
 def bench_reconnect(args, ov, tangle, p):

@@ -243,6 +243,17 @@ int ov_get_rk4_classic(void);
 void ov_set_mixed_near_factor(double factor);
 double ov_get_mixed_near_factor(void);
 
+/* The colinearity cut-off of the segment formula: a segment adds nothing
+ * where |cos(R, R') - 1| < eps (the reference's eps = 1e-8,
+ * src/tangle.c:505-506, the default).  It makes the velocity discontinuous
+ * where a segment's extension passes near a target.  eps = 0 switches it
+ * off in the FP64 direct sums and in the adjoint (ov_adjoint_*), for
+ * gradient checks against finite differences of a smooth function; the
+ * Barnes-Hut walks and the mixed form keep the reference's value.  Not the
+ * reference's behaviour when changed.  Captured when a tangle is uploaded. */
+void ov_set_colinear_cutoff(double eps);
+double ov_get_colinear_cutoff(void);
+
 /* Per-call counters of the last velocity evaluation on this thread. */
 typedef struct {
   double interactions;      /* segment-point interactions (direct and P2P) */

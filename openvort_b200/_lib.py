@@ -31,7 +31,8 @@ FUNCTIONS = [
     "ov_state_update_tangle", "ov_state_rk4_step", "ov_state_run", "ov_state_eval_points",
     "ov_measure_fma_peak", "ov_state_get_stats", "ov_state_reset_stats", "ov_state_shard",
     "ov_state_shard_bytes", "ov_state_shard_begin", "ov_state_shard_end",
-    "ov_set_mixed_near_factor", "ov_get_mixed_near_factor", "ov_direct_points_noalloc",
+    "ov_set_mixed_near_factor", "ov_get_mixed_near_factor", "ov_set_colinear_cutoff",
+    "ov_get_colinear_cutoff", "ov_direct_points_noalloc",
     "ov_batch_create", "ov_batch_destroy", "ov_batch_update", "ov_batch_run",
     "ov_batch_download", "ov_batch_set_tuning", "ov_batch_get_tuning", "ov_batch_autotune",
     "ov_batch_get_stats", "ov_adjoint_create", "ov_adjoint_destroy", "ov_adjoint_velocity",
@@ -168,6 +169,8 @@ def load(path: os.PathLike | str | None = None) -> C.CDLL:
         "ov_reconnect_candidates": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p, C.c_int]),
         "ov_reconnect_vortices": (C.c_int, [T, C.c_double, C.c_double, C.c_double]),
         "ov_reconnect_get_stats": (C.c_int, [C.POINTER(ReconnectStats)]),
+        "ov_set_colinear_cutoff": (None, [C.c_double]),
+        "ov_get_colinear_cutoff": (C.c_double, []),
         "ov_remesh": (C.c_int, [T, C.c_double, C.c_double, C.c_void_p]),
         "ov_enforce_boundaries": (C.c_int, [T]),
         "ov_eliminate_small_loops": (C.c_int, [T, C.c_int]),

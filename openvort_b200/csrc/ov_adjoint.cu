@@ -157,16 +157,16 @@ __global__ void k_local_vjp(LocalP L, const double* __restrict__ pos, const int2
 // Q = P + R.R', a = |R|, b = |R'|, R = r1 - r, R' = r2 - r.  Given g, the
 // cotangents of R and R' of g . v; zero where the reference's cut-offs
 // return zero.
-__device__ __forceinline__ void seg_vjp(double f4pi, d3 r1, d3 r2, d3 r, d3 g, d3& Rb, d3& Rpb) {
+__device__ __forceinline__ void seg_vjp(double f4pi, double col, d3 r1, d3 r2, d3 r, d3 g, d3& Rb, d3& Rpb) {
   Rb = Rpb = mk3(0, 0, 0);
   const d3 R = r1 - r, Rp = r2 - r;
   const double a = sqrt(dot3(R, R)), b = sqrt(dot3(Rp, Rp));
   const double RRp = dot3(R, Rp);
   if (a < 1e-8 || b < 1e-8) return;
   const double P = a * b;
-  if (fabs(RRp / P - 1.0) < 2e-8) {
+  if (fabs(RRp / P - 1.0) < 2.0 * col) {
     const double cref = __ddiv_rn(__ddiv_rn(RRp, a), b);
-    if (fabs(cref - 1.0) < 1e-8) return;
+    if (fabs(cref - 1.0) < col) return;
   }
   const double Q = P + RRp;
   const double s = f4pi * (a + b) / (P * Q);
@@ -189,7 +189,7 @@ constexpr int kVT = 128;   // threads per block and tile length
 // Pass A: per target k, x_bar_k -= sum_m (Rb + Rpb) over the segments
 // (r = x_k enters R and R' with a minus sign); skip rule of
 // calculate_vs_shift (src/tangle.c:567-569).
-__global__ void __launch_bounds__(kVT) k_bs_vjp_targets(double f4pi, const double* __restrict__ pos,
+__global__ void __launch_bounds__(kVT) k_bs_vjp_targets(double f4pi, double col, const double* __restrict__ pos,
                                                         const int2* __restrict__ links,
                                                         const int2* __restrict__ status,
                                                         const double* __restrict__ gnl, double* xbar,
@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_targets(double f4pi, const doubl
       const int id = sid[q][0], fw = sid[q][1];
       if (fw < 0 || id == k || fw == k) continue;
       d3 Rb, Rpb;
-      seg_vjp(f4pi, mk3(sh[q][0], sh[q][1], sh[q][2]), mk3(sh[q][3], sh[q][4], sh[q][5]), r, g, Rb, Rpb);
+      seg_vjp(f4pi, col, mk3(sh[q][0], sh[q][1], sh[q][2]), mk3(sh[q][3], sh[q][4], sh[q][5]), r, g, Rb, Rpb);
       acc = acc - (Rb + Rpb);
     }
   }
@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_targets(double f4pi, const doubl
 
 // Pass B: per segment m (x_m -> x_fwd), sum over the targets of Rb (to x_m)
 // and Rpb (to x_fwd).
-__global__ void __launch_bounds__(kVT) k_bs_vjp_segments(double f4pi, const double* __restrict__ pos,
+__global__ void __launch_bounds__(kVT) k_bs_vjp_segments(double f4pi, double col, const double* __restrict__ pos,
                                                          const int2* __restrict__ links,
                                                          const int2* __restrict__ status,
                                                          const double* __restrict__ gnl, double* xbar,
@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(kVT) k_bs_vjp_segments(double f4pi, const doub
       const int kk = sid[q];
       if (kk < 0 || kk == m || kk == f) continue;
       d3 Rb, Rpb;
-      seg_vjp(f4pi, r1, r2, mk3(sh[q][0], sh[q][1], sh[q][2]), mk3(sh[q][3], sh[q][4], sh[q][5]), Rb, Rpb);
+      seg_vjp(f4pi, col, r1, r2, mk3(sh[q][0], sh[q][1], sh[q][2]), mk3(sh[q][3], sh[q][4], sh[q][5]), Rb, Rpb);
       a1 = a1 + Rb;
       a2 = a2 + Rpb;
     }
@@ -390,10 +390,10 @@ bool velocity_vjp(ov_adjoint* a, const double* x, const double* g, double* ybar)
     int splits = 1;
     const int chunk = pair_chunk(n, &splits);
     const dim3 grid(blocks(n, kVT), splits);
-    k_bs_vjp_targets<<<grid, kVT, 0, s->stream>>>(s->P.f4pi, x, s->links.as<int2>(), s->status.as<int2>(),
+    k_bs_vjp_targets<<<grid, kVT, 0, s->stream>>>(s->P.f4pi, s->P.col_cut, x, s->links.as<int2>(), s->status.as<int2>(),
                                                   a->gnl.as<double>(), ybar, n, chunk);
     OV_LAUNCHED();
-    k_bs_vjp_segments<<<grid, kVT, 0, s->stream>>>(s->P.f4pi, x, s->links.as<int2>(), s->status.as<int2>(),
+    k_bs_vjp_segments<<<grid, kVT, 0, s->stream>>>(s->P.f4pi, s->P.col_cut, x, s->links.as<int2>(), s->status.as<int2>(),
                                                    a->gnl.as<double>(), ybar, n, chunk);
     OV_LAUNCHED();
   }

@@ -140,6 +140,7 @@ int g_rk4_classic = 0;
 // at 4 or 16) the mixed velocities stay within ~3e-6 of the FP64 ones on the
 // benchmark tangles
 double g_near_factor = 8.0;
+double g_col_cut = 1e-8;   // the reference's colinearity cut-off (src/tangle.c:505)
 int g_device = -1;
 std::mutex g_init_mutex;
 }  // namespace
@@ -218,6 +219,8 @@ int ov_get_precision(void) { return g_precision; }
 void ov_set_rk4_classic(int classic) { g_rk4_classic = classic ? 1 : 0; }
 void ov_set_mixed_near_factor(double f) { g_near_factor = f > 0 ? f : 0; }
 double ov_get_mixed_near_factor(void) { return g_near_factor; }
+void ov_set_colinear_cutoff(double eps) { g_col_cut = eps > 0 ? eps : 0; }
+double ov_get_colinear_cutoff(void) { return g_col_cut; }
 int ov_get_rk4_classic(void) { return g_rk4_classic; }
 
 int ov_init(int device) {
@@ -369,6 +372,7 @@ bool capture_params(const tangle_state* t, OvParams& P, bool need_flows) {
   P.alpha_p = global_alpha_p;
   P.max_curv = global_max_curvature_scale;
   P.hyperalpha = global_hyperalpha;
+  P.col_cut = g_col_cut;
   if (need_flows) {
     if (!parse_flow(vs_conf, "vs_conf", P.vs)) return false;
     if (P.use_mf && !parse_flow(vn_conf, "vn_conf", P.vn)) return false;

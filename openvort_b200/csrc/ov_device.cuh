@@ -44,6 +44,9 @@ struct OvParams {
   double theta, grain, dl_max;
   double near2;                 // mixed form: squared radius of the FP64 near field
   double alpha, alpha_p, max_curv, hyperalpha;
+  // colinearity cut-off of the FP64 direct sums and the adjoint: the
+  // reference's 1e-8 (src/tangle.c:505), 0 switches it off
+  double col_cut;
   OvFlow vn, vs, vb;
 };
 
@@ -129,7 +132,7 @@ __device__ __forceinline__ d3 mirror_dir(d3 v, int face) {
 
 // FP64, the reference's formula and cut-offs: zero when either endpoint is
 // closer than 1e-8 or R, R' are colinear to 1e-8.
-__device__ __forceinline__ d3 seg_vel64(double f4pi, d3 r1, d3 r2, d3 r) {
+__device__ __forceinline__ d3 seg_vel64(double f4pi, d3 r1, d3 r2, d3 r, double col = 1e-8) {
   d3 R = r1 - r, Rp = r2 - r;
   double R2 = dot3(R, R), Rp2 = dot3(Rp, Rp);
   double lR = sqrt(R2), lRp = sqrt(Rp2);
@@ -140,9 +143,9 @@ __device__ __forceinline__ d3 seg_vel64(double f4pi, d3 r1, d3 r2, d3 r) {
   // when the cheap estimate is within a factor 2 of the threshold
   double c = RRp / p;
   double e = fabs(c - 1.0);
-  if (e < 2e-8) {
+  if (e < 2.0 * col) {
     double cref = __ddiv_rn(__ddiv_rn(RRp, lR), lRp);
-    if (fabs(cref - 1.0) < 1e-8) return mk3(0, 0, 0);
+    if (fabs(cref - 1.0) < col) return mk3(0, 0, 0);
   }
   double s = f4pi * (lR + lRp) / (p * (p + RRp));
   return cross3(R, Rp) * s;
@@ -183,14 +186,14 @@ __device__ __forceinline__ double rcp_nr(double x) {
 // of |R'|.  Where either cut-off could decide (|R| or |R'| within 1.5x of
 // 1e-8, or cos within 2e-8 of 1) the reference's own operations decide
 // (seg_vel64), so every cut-off decision is the reference's.
-__device__ __forceinline__ d3 seg_vel64_nr(double f4pi, d3 r1, d3 r2, d3 d, d3 r) {
+__device__ __forceinline__ d3 seg_vel64_nr(double f4pi, d3 r1, d3 r2, d3 d, d3 r, double col = 1e-8) {
   const d3 R = r1 - r;
   const d3 Rp = R + d;
   const double R2 = dot3(R, R), Rp2 = dot3(Rp, Rp), RRp = dot3(R, Rp);
-  if (R2 < 2.25e-16 || Rp2 < 2.25e-16) return seg_vel64(f4pi, r1, r2, r);
+  if (R2 < 2.25e-16 || Rp2 < 2.25e-16) return seg_vel64(f4pi, r1, r2, r, col);
   const double ia = rsqrt_nr(R2), ib = rsqrt_nr(Rp2);
   const double u = ia * ib;
-  if (fabs(fma(RRp, u, -1.0)) < 2e-8) return seg_vel64(f4pi, r1, r2, r);
+  if (fabs(fma(RRp, u, -1.0)) < 2.0 * col) return seg_vel64(f4pi, r1, r2, r, col);
   const double s = f4pi * (ia + ib) * (u * rcp_nr(fma(RRp, u, 1.0)));
   return cross3(R, Rp) * s;
 }

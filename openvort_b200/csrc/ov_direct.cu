@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(kTB) k_direct64(OvParams P, SegTab S, int n_sr
       if (fw == -1 || id == skip || fw == skip) continue;
       d3 v = seg_vel64_nr(f4pi, mk3(sh_r[q][0], sh_r[q][1], sh_r[q][2]),
                           mk3(sh_r[q][3], sh_r[q][4], sh_r[q][5]),
-                          mk3(sh_r[q][6], sh_r[q][7], sh_r[q][8]), r);
+                          mk3(sh_r[q][6], sh_r[q][7], sh_r[q][8]), r, P.col_cut);
       ax += v.x; ay += v.y; az += v.z;
     }
   }
@@ -197,8 +197,8 @@ __global__ void __launch_bounds__(kTB) k_direct64_chain(OvParams P, SegTab S, in
         d3 v;
         const double RRp = dot3(Ra, Rb);
         const double u = ia * ib;
-        if (Ra2 < 2.25e-16 || Rb2 < 2.25e-16 || fabs(fma(RRp, u, -1.0)) < 2e-8) {
-          v = seg_vel64(f4pi, mk3(sh_node[i][0], sh_node[i][1], sh_node[i][2]), nb, r);
+        if (Ra2 < 2.25e-16 || Rb2 < 2.25e-16 || fabs(fma(RRp, u, -1.0)) < 2.0 * P.col_cut) {
+          v = seg_vel64(f4pi, mk3(sh_node[i][0], sh_node[i][1], sh_node[i][2]), nb, r, P.col_cut);
         } else {
           const double sc = f4pi * (ia + ib) * (u * rcp_nr(fma(RRp, u, 1.0)));
           v = cross3(Ra, Rb) * sc;
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kTB) k_direct64_chain(OvParams P, SegTab S, in
       if (m == skip || fw == skip) continue;
       const double* sg = S.r1r2 + 6 * (size_t)m;
       const d3 r1 = mk3(sg[0], sg[1], sg[2]), r2 = mk3(sg[3], sg[4], sg[5]);
-      const d3 v = seg_vel64_nr(f4pi, r1, r2, r2 - r1, r);
+      const d3 v = seg_vel64_nr(f4pi, r1, r2, r2 - r1, r, P.col_cut);
       ax += v.x;
       ay += v.y;
       az += v.z;

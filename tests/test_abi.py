@@ -130,6 +130,9 @@ def test_global_defaults(lib):
         ref = C.CDLL(str(REF_SO))
         for sym, attr, ctype in Params.GLOBALS:
             assert ctype.in_dll(ref, sym).value == ctype.in_dll(lib, sym).value, sym
+    # the colinearity cut-off of the segment formula (src/tangle.c:505-506)
+    lib.ov_get_colinear_cutoff.restype = C.c_double
+    assert lib.ov_get_colinear_cutoff() == 1e-8
 
 
 def test_error_strings(lib):
