@@ -178,6 +178,22 @@ __global__ void k_rec_scatter(const int* __restrict__ nodes, int count, int n, c
   st3(v_img, k, ld3(img, i));
 }
 
+// the four links do_reconnection changed, as kernel arguments
+struct LinkPatch {
+  int slot[4];
+  int2 link[4];
+};
+
+__global__ void k_rec_patch_links(LinkPatch L, int2* links, int n, int* flag) {
+  const int c = threadIdx.x;
+  if (c >= 4) return;
+  if (L.slot[c] < 0 || L.slot[c] >= n) {
+    atomicOr(flag, 1);
+    return;
+  }
+  links[L.slot[c]] = L.link[c];
+}
+
 // one segment change of a reconnection: slot m's forward link was (sign -1)
 // or is now (sign +1) f
 struct SegChange {
@@ -187,33 +203,52 @@ struct SegChange {
 
 // v_nl and v_img of the listed nodes += the changed segments' fields, with
 // the skip rule of the tangle's own sum (src/tangle.c:614-616) and the
-// mirror reflection of each image's sum (src/tangle.c:633-634)
-__global__ void k_rec_correct(OvParams P, SegChange C, const int* __restrict__ nodes, int count, int n,
-                              const double* __restrict__ pos, double* v_nl, double* v_img, int* flag) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
+// mirror reflection of each image's sum (src/tangle.c:633-634).  One warp
+// per node: lane 0 takes the tangle itself, the lanes share the images
+// (image j on lane j mod 32), and the image terms are added in a fixed
+// shuffle tree, so the result does not depend on scheduling.
+constexpr int kCorrectWarps = 4;
+__global__ void __launch_bounds__(32 * kCorrectWarps) k_rec_correct(OvParams P, SegChange C,
+                                                                   const int* __restrict__ nodes, int count,
+                                                                   int n, const double* __restrict__ pos,
+                                                                   double* v_nl, double* v_img, int* flag) {
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kCorrectWarps + (threadIdx.x >> 5);
+  if (i >= count) return;   // whole warp
   const int k = nodes[i];
   bool ok = k >= 0 && k < n;
   for (int c = 0; c < 4; ++c) ok = ok && C.m[c] >= 0 && C.m[c] < n && C.f[c] >= 0 && C.f[c] < n;
   if (!ok) {
-    atomicOr(flag, 1);
+    if (lane == 0) atomicOr(flag, 1);
     return;
   }
   const d3 r = ld3(pos, k);
-  d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
+  d3 r1[4], r2[4];
   for (int c = 0; c < 4; ++c) {
-    const d3 r1 = ld3(pos, C.m[c]);
-    const d3 r2 = pwrap(P, r1, ld3(pos, C.f[c]));
-    if (k != C.m[c] && k != C.f[c]) nl = nl + seg_vel64(P.f4pi, r1, r2, r) * C.sign[c];
-    for (int j = 0; j < P.n_img; ++j) {
-      d3 v = seg_vel64(P.f4pi, r1, r2, image_point(P, j, r)) * C.sign[c];
-      const int face = P.img[j][3];
-      if (face > -1) v = mirror_dir(v, face);
-      im = im + v;
-    }
+    r1[c] = ld3(pos, C.m[c]);
+    r2[c] = pwrap(P, r1[c], ld3(pos, C.f[c]));
   }
-  st3(v_nl, k, ld3(v_nl, k) + nl);
-  st3(v_img, k, ld3(v_img, k) + im);
+  d3 nl = mk3(0, 0, 0), im = mk3(0, 0, 0);
+  if (lane == 0)
+    for (int c = 0; c < 4; ++c)
+      if (k != C.m[c] && k != C.f[c]) nl = nl + seg_vel64(P.f4pi, r1[c], r2[c], r) * C.sign[c];
+  for (int j = lane; j < P.n_img; j += 32) {
+    const d3 t = image_point(P, j, r);
+    d3 v = mk3(0, 0, 0);
+    for (int c = 0; c < 4; ++c) v = v + seg_vel64(P.f4pi, r1[c], r2[c], t) * C.sign[c];
+    const int face = P.img[j][3];
+    if (face > -1) v = mirror_dir(v, face);
+    im = im + v;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    im.x += __shfl_down_sync(0xffffffffu, im.x, off);
+    im.y += __shfl_down_sync(0xffffffffu, im.y, off);
+    im.z += __shfl_down_sync(0xffffffffu, im.z, off);
+  }
+  if (lane == 0) {
+    st3(v_nl, k, ld3(v_nl, k) + nl);
+    st3(v_img, k, ld3(v_img, k) + im);
+  }
 }
 
 // vels and vs of the listed nodes, packed 6 doubles per node for one copy
@@ -231,7 +266,29 @@ __global__ void k_rec_pack(const int* __restrict__ nodes, int count, int n, cons
   st3(out + 6 * (size_t)i + 3, 0, ld3(vs, k));
 }
 
+// Pinned host memory for the pass's per-reconnection copies (the known list
+// up, the known nodes' values and the error flag down), so each copy is one
+// asynchronous transfer rather than a staged pageable one.
+struct PinnedBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  bool reserve(size_t n) {
+    if (n <= bytes) return true;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    if (!ov_cuda_ok(cudaMallocHost(&p, n), "cudaMallocHost")) return false;
+    bytes = n;
+    return true;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+  ~PinnedBuf() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
 struct RecState {
+  PinnedBuf h_list, h_vals;   // known list (ints), known values (6 doubles each) + flag
   ov_state_impl s;
   DevBuf keys, keys2, ids, ids2, pairs, count, hist, scan_part, skip, pack;
   DevBuf batch, pts, bnl, bimg, known;   // batched velocities
@@ -404,18 +461,29 @@ bool refresh_known(RecState& R, RecVel& V) {
                                                        s->vs.as<double>(), R.pack.as<double>(), flag);
   OV_LAUNCHED();
   OV_TRY_CUDA(cudaGetLastError());
-  int h_flag = 0;
-  V.hv.resize(6 * (size_t)cnt);
-  OV_TRY_CUDA(cudaMemcpyAsync(V.hv.data(), R.pack.p, sizeof(double) * 6 * (size_t)cnt, cudaMemcpyDeviceToHost,
-                              s->stream));
-  OV_TRY_CUDA(cudaMemcpyAsync(&h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  // the values, then the flag, into pinned memory: one wait
+  const size_t vbytes = sizeof(double) * 6 * (size_t)cnt;
+  if (!R.h_vals.reserve(vbytes + 64)) return false;
+  int* h_flag = reinterpret_cast<int*>(R.h_vals.as<char>() + vbytes);
+  OV_TRY_CUDA(cudaMemcpyAsync(R.h_vals.p, R.pack.p, vbytes, cudaMemcpyDeviceToHost, s->stream));
+  OV_TRY_CUDA(cudaMemcpyAsync(h_flag, flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
-  return ov_flag_status(h_flag, "update_velocity");
+  V.hv.assign(R.h_vals.as<double>(), R.h_vals.as<double>() + 6 * (size_t)cnt);
+  return ov_flag_status(*h_flag, "update_velocity");
 }
 
-// Nonlocal and image sums of new nodes on the current links (one batched
-// FP64 direct sum), added to the known set; then every known node's
-// epilogue and host copy.
+// the known list to the device (R.known), through pinned memory.  Every
+// upload is followed by refresh_known's wait before the next one, so the
+// pinned list is never rewritten while a copy from it is in flight.
+bool upload_known(RecState& R, const RecVel& V) {
+  const size_t cnt = V.known.size();
+  if (cnt == 0) return true;
+  if (!R.known.reserve(sizeof(int) * cnt) || !R.h_list.reserve(sizeof(int) * cnt)) return false;
+  std::copy(V.known.begin(), V.known.end(), R.h_list.as<int>());
+  OV_TRY_CUDA(cudaMemcpyAsync(R.known.p, R.h_list.p, sizeof(int) * cnt, cudaMemcpyHostToDevice, R.s.stream));
+  return true;
+}
+
 // Nonlocal and image sums of the m nodes at `batch` (a device list) on the
 // current links into v_nl, v_img: FP64, or (mixed) the FP32 far field with
 // a bound on its error per node copied into hb.
@@ -444,6 +512,8 @@ bool sum_nodes(RecState& R, const int* batch, int m, bool mixed, double* hb) {
   return true;
 }
 
+// Sums of new nodes on the current links (one batched direct sum), added to
+// the known set; then every known node's epilogue and host copy.
 bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes, bool mixed) {
   ov_state_impl* s = &R.s;
   const int m = (int)nodes.size();
@@ -455,10 +525,8 @@ bool compute_nodes(RecState& R, RecVel& V, const std::vector<int>& nodes, bool m
   }
   const int cnt = (int)V.known.size();
   V.bound.resize(cnt, 0.0);
-  if (!R.known.reserve(sizeof(int) * (size_t)cnt)) return false;
   // the whole list: growing R.known reallocates it without its contents
-  OV_TRY_CUDA(cudaMemcpyAsync(R.known.as<int>(), V.known.data(), sizeof(int) * (size_t)cnt,
-                              cudaMemcpyHostToDevice, s->stream));
+  if (!upload_known(R, V)) return false;
   const auto t0 = std::chrono::steady_clock::now();
   if (!s->P.lia_only && !sum_nodes(R, R.known.as<int>() + old, m, mixed, V.bound.data() + old)) return false;
   OV_TRY_CUDA(cudaStreamSynchronize(s->stream));
@@ -625,12 +693,15 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     old_fwd[0] = changed[0] == k ? knext : lnext;
     old_fwd[1] = changed[0] == k ? l : k;
     // the same links on the device
-    for (int c = 0; c < 4; ++c) {
-      const int m = changed[c];
-      if (!ov_cuda_ok(cudaMemcpyAsync(s->links.as<int2>() + m, &tangle->connections[m], sizeof(int2),
-                                      cudaMemcpyHostToDevice, s->stream),
-                      "cudaMemcpyAsync"))
-        return -ov_last_error();
+    {
+      LinkPatch L;
+      for (int c = 0; c < 4; ++c) {
+        L.slot[c] = changed[c];
+        L.link[c] = make_int2(tangle->connections[changed[c]].forward, tangle->connections[changed[c]].reverse);
+      }
+      k_rec_patch_links<<<1, 32, 0, s->stream>>>(L, s->links.as<int2>(), s->n, s->dflag.as<int>());
+      OV_LAUNCHED();
+      if (!ov_cuda_ok(cudaGetLastError(), "k_rec_patch_links")) return -ov_last_error();
     }
     const int flag[10] = {k, tangle->connections[k].forward, tangle->connections[k].reverse, knext, kprev,
                           l, tangle->connections[l].forward, tangle->connections[l].reverse, lnext, lprev};
@@ -657,11 +728,7 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
       }
       V.known.swap(keep);
       V.bound.swap(keep_bound);
-      if (!V.known.empty() &&
-          !ov_cuda_ok(cudaMemcpyAsync(R.known.as<int>(), V.known.data(), sizeof(int) * V.known.size(),
-                                      cudaMemcpyHostToDevice, s->stream),
-                      "cudaMemcpyAsync"))
-        return -ov_last_error();
+      if (!upload_known(R, V)) return -ov_last_error();
     }
     // every known node: the removed and added segments' fields
     SegChange C;
@@ -671,9 +738,9 @@ int ov_reconnect_vortices(struct tangle_state* tangle, double t, double rec_dist
     C.m[3] = changed[3]; C.f[3] = tangle->connections[changed[3]].forward; C.sign[3] = 1;
     const int cnt = (int)V.known.size();
     if (cnt > 0 && !s->P.lia_only) {
-      k_rec_correct<<<(cnt + 127) / 128, 128, 0, s->stream>>>(s->P, C, R.known.as<int>(), cnt, s->n,
-                                                               s->pos.as<double>(), s->v_nl.as<double>(),
-                                                               s->v_img.as<double>(), s->dflag.as<int>());
+      k_rec_correct<<<(cnt + kCorrectWarps - 1) / kCorrectWarps, 32 * kCorrectWarps, 0, s->stream>>>(
+          s->P, C, R.known.as<int>(), cnt, s->n, s->pos.as<double>(), s->v_nl.as<double>(),
+          s->v_img.as<double>(), s->dflag.as<int>());
       OV_LAUNCHED();
       if (!ov_cuda_ok(cudaGetLastError(), "k_rec_correct")) return -ov_last_error();
     }
