@@ -65,6 +65,10 @@ def fixture_flows(meta: dict):
 # its seed; samples/cfg2_bh4.npz holds the reference's velocities at seeded
 # sample nodes of it and a checksum of its positions.
 CFG2 = {"seed": 2026, "rings": 512, "D": 0.1, "dl": 0.1 / 200, "samples": 256}
+# further seeds of the same workload (samples/cfg2_bh4_s<seed>.npz), fewer
+# sample nodes each
+CFG2_SEEDS = (0, 1, 2, 3, 4)
+CFG2_SEED_SAMPLES = 64
 
 
 def cfg2_params(use_bh: int) -> Params:
@@ -73,16 +77,21 @@ def cfg2_params(use_bh: int) -> Params:
                   vn=Flow("simple", {"external_v": (0.5, 0.0, 0.0)}), vs=Flow("no flow"))
 
 
-def cfg2_tangle():
-    return G.random_ring_tangle(CFG2["seed"], CFG2["rings"], CFG2["D"], dl=CFG2["dl"], boundary="periodic-26")
+def cfg2_tangle(seed: int | None = None):
+    seed = CFG2["seed"] if seed is None else seed
+    return G.random_ring_tangle(seed, CFG2["rings"], CFG2["D"], dl=CFG2["dl"], boundary="periodic-26")
 
 
-def load_cfg2_samples():
+def cfg2_sample_name(seed: int | None = None) -> str:
+    return "cfg2_bh4" if seed is None else f"cfg2_bh4_s{seed}"
+
+
+def load_cfg2_samples(seed: int | None = None):
     """(tangle, sample fixture); asserts the regenerated tangle is the one
     the reference ran on."""
-    z = np.load(GOLDEN / "samples" / "cfg2_bh4.npz")
+    z = np.load(GOLDEN / "samples" / (cfg2_sample_name(seed) + ".npz"))
     meta = json.loads(str(z["meta"]))
-    t = cfg2_tangle()
+    t = cfg2_tangle(seed)
     assert t.n == meta["n"] and float(np.sum(t.pos)) == meta["pos_sum"] and \
         float(np.sum(np.abs(t.pos))) == meta["pos_abs_sum"], "generator no longer reproduces the tangle"
     return t, z

@@ -34,7 +34,7 @@ from openvort_b200.tangle import Flow, Params  # noqa: E402
 from oracle.oracle import Ref, build  # noqa: E402
 
 sys.path.insert(0, str(ROOT / "tests"))
-from cases import CFG2, cfg2_params, cfg2_tangle  # noqa: E402
+from cases import CFG2, CFG2_SEED_SAMPLES, CFG2_SEEDS, cfg2_params, cfg2_sample_name, cfg2_tangle  # noqa: E402
 
 OUT = Path(__file__).resolve().parent
 
@@ -134,15 +134,16 @@ def flows16(ref):
     print("flows16", t.n, "nodes")
 
 
-def cfg2_samples(ref):
+def cfg2_samples(ref, seed=None):
     """The 22.4k-point periodic tangle of the config-2 workload (regenerated
     by the tests from its seed; a checksum pins it): the reference's vs
     (update_velocity: local term, flow, Biot-Savart, 26 images) at seeded
     sample nodes with its octree at theta 0.4 and with its direct sum."""
     import ctypes as C
-    t = cfg2_tangle()
-    rng = np.random.default_rng(CFG2["seed"])
-    idx = np.sort(rng.choice(np.nonzero(t.active)[0], size=CFG2["samples"], replace=False)).astype(np.int32)
+    t = cfg2_tangle(seed)
+    rng = np.random.default_rng(CFG2["seed"] if seed is None else seed)
+    size = CFG2["samples"] if seed is None else CFG2_SEED_SAMPLES
+    idx = np.sort(rng.choice(np.nonzero(t.active)[0], size=size, replace=False)).astype(np.int32)
     out = {}
     for name, use_bh in (("vs_bh4", 1), ("vs_direct", 0)):
         p = cfg2_params(use_bh)
@@ -159,10 +160,12 @@ def cfg2_samples(ref):
         tb = C.c_double()
         f(C.cast(tt.ptr(), C.c_void_p), 0.0, idx.ctypes.data, len(idx), use_bh, v.ctypes.data, C.byref(tb))
         out[name] = v
-    meta = {**CFG2, "n": t.n, "pos_sum": float(np.sum(t.pos)), "pos_abs_sum": float(np.sum(np.abs(t.pos)))}
+    meta = {**CFG2, "seed": CFG2["seed"] if seed is None else seed, "samples": size, "n": t.n,
+            "pos_sum": float(np.sum(t.pos)), "pos_abs_sum": float(np.sum(np.abs(t.pos)))}
     (OUT / "samples").mkdir(exist_ok=True)
-    np.savez_compressed(OUT / "samples" / "cfg2_bh4.npz", meta=np.array(json.dumps(meta)), idx=idx, **out)
-    print("cfg2_bh4 samples", t.n, "nodes")
+    name = cfg2_sample_name(seed)
+    np.savez_compressed(OUT / "samples" / (name + ".npz"), meta=np.array(json.dumps(meta)), idx=idx, **out)
+    print(name, "samples", t.n, "nodes")
 
 
 def main():
@@ -173,6 +176,9 @@ def main():
         flows16(ref)
     if not only or "cfg2_bh4" in only:
         cfg2_samples(ref)
+    for seed in CFG2_SEEDS:
+        if not only or cfg2_sample_name(seed) in only:
+            cfg2_samples(ref, seed)
     for name, t, p, opt in cases():
         if only and name not in only:
             continue

@@ -128,6 +128,21 @@ def test_config2_tangle_bh4_and_direct_vs_reference(ov):
         assert rel_err(mixed.vs[idx], z[key]) < TOL_MIXED, key
 
 
+@pytest.mark.parametrize("seed", [0, 1, 2, 3, 4])
+def test_config2_seeds_bh4_and_direct_vs_reference(ov, seed):
+    """Config 2's seeds 0..4 (22.5k-22.8k points each): FP64 Barnes-Hut
+    (theta 0.4) and direct sums against the reference's update_velocity at
+    64 sample nodes per tangle, and the mixed form within its tolerance."""
+    from cases import cfg2_params, load_cfg2_samples
+    t, z = load_cfg2_samples(seed)
+    idx = z["idx"]
+    for use_bh, key in ((1, "vs_bh4"), (0, "vs_direct")):
+        out = gpu_update(ov, t, cfg2_params(use_bh))
+        assert rel_err(out.vs[idx], z[key]) < TOL_V64, key
+        mixed = gpu_update(ov, t, cfg2_params(use_bh), precision=1)
+        assert rel_err(mixed.vs[idx], z[key]) < TOL_MIXED, key
+
+
 def test_refined_fp64_reciprocals_match_ieee(ov):
     """The direct sum's FP64 1/sqrt(x) and 1/x (hardware approximation plus
     two Newton-Raphson steps) stay within 4 ulps of IEEE sqrt and division

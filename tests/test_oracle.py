@@ -60,6 +60,14 @@ def test_oracle_bh4_on_the_config2_tangle(oracle):
     assert rel_err(z["vs_bh4"], z["vs_direct"]) > 1e-4
 
 
+def test_oracle_bh4_on_another_config2_seed(oracle):
+    """The same on config 2's seed 3 (64 sample nodes)."""
+    from cases import cfg2_params, load_cfg2_samples
+    t, z = load_cfg2_samples(3)
+    out = oracle.update_tangle(t, cfg2_params(1))
+    assert rel_err(out.vs[z["idx"]], z["vs_bh4"]) < TOL_V
+
+
 def test_bh_differs_from_direct(oracle):
     """The Barnes-Hut fixtures exercise the tree: their error against the
     direct sum is the reference's BH error, orders above the parity bound."""
