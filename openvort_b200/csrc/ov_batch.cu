@@ -98,23 +98,28 @@ __global__ void __launch_bounds__(TB) k_batch_bs64(OvParams P, BatchView B,
   }
 }
 
-// Mixed form: two-float FP32 offsets from the item's first target (the
-// systems' targets and sources span whole rings, so a single rounding of
-// the offsets would cost a near segment ~1e-6 of its |R|), two sources per
+// Mixed form: FP32 offsets from one origin per work item.  Items of 64
+// threads (128 targets at two per thread) take single-rounded offsets from
+// the item's middle target: the items span at most 64 node spacings either
+// side, and the
+// measured error against the FP64 form is 3.8e-6 on the 4096-system bench
+// ensemble.  Larger items take two-float offsets (hi + lo) from their first
+// target (error 8e-8), since a single rounding over a whole ring would cost a
+// near segment ~1e-6 of its |R|.  Two sources per
 // f32x2 instruction and kTT targets per thread (pair_interact); pairs
 // nearer than max(4 |ds|, the system's near radius) or too close to the
 // colinearity cut-off take the FP64 formula from the FP64 positions.  FP32
 // partial sums over 32 sources are added into FP64 sums.  With open
 // boundaries the two segments the skip rule drops have an endpoint at the
 // target, so they are near and the FP64 cut-off returns zero for them.
-template <int TB, int TS>
+template <int TB, int TS, bool kTwo = (TB > 64)>
 __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
                                                        const double* __restrict__ pos,
                                                        const int2* __restrict__ links,
                                                        const int2* __restrict__ status,
                                                        StoreSums out, int* __restrict__ work) {
   static_assert(TS % 32 == 0, "sources per tile");
-  __shared__ PairSrc<true> sh[TS / 2];
+  __shared__ PairSrc<kTwo> sh[TS / 2];
   __shared__ int sh_item;
   const double f4pi = P.f4pi;
   for (;;) {
@@ -126,7 +131,9 @@ __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
     const int2 w = B.items[it];
     const int s0 = B.off[w.x], s1 = B.off[w.x + 1];
     const double near2 = B.near2[w.x];
-    const d3 O = ld3(pos, w.y);
+    // two-float offsets from the item's first target; single-rounded ones
+    // from its middle target
+    const d3 O = ld3(pos, kTwo ? w.y : w.y + min(TB * kTT, s1 - w.y) / 2);
     int kk[kTT];
     PairTargets T;
     double acc[kTT][3];
@@ -172,7 +179,7 @@ __global__ void __launch_bounds__(TB) k_batch_bs_mixed(OvParams P, BatchView B,
         for (int k = 0; k < kTT; ++k) bsum[k][0] = bsum[k][1] = bsum[k][2] = f2_splat(0.f);
         const int q1 = min(q0 + 16, nrec);
 #pragma unroll 2
-        for (int q = q0; q < q1; ++q) pair_interact<true>(sh[q], T, bsum, special);
+        for (int q = q0; q < q1; ++q) pair_interact<kTwo>(sh[q], T, bsum, special);
 #pragma unroll
         for (int k = 0; k < kTT; ++k) {
 #pragma unroll
