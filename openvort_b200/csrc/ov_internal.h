@@ -79,6 +79,7 @@ __host__ __device__ __forceinline__ int cell_lbot(int meta) { return (meta >> 16
 
 struct OvTree {
   int n_nodes = 0;      // active (non-EMPTY) nodes
+  int n_drop_root = 0;  // active nodes outside the root box (sorted last)
   int n_cells = 0;
   int built = 0;
   double theta = 0;     // theta used for thr
@@ -95,6 +96,7 @@ struct OvTree {
   DevBuf scratch;
   DevBuf scan_part;     // block sums of the exclusive scans
   DevBuf mom_part;      // per-chunk partial moments of the largest cells
+  DevBuf walk_order;    // the walk's target list when nodes lie outside the root box
 };
 
 // ---------------------------------------------------------------- state

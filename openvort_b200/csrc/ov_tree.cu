@@ -131,7 +131,12 @@ __global__ void k_keys(OvParams P, const double* __restrict__ pos, const int2* _
     }
     ++level;
     set_digit(h, l, level, digit);
-    if (digit == kDigitDropped) { tl = level - 1; tk = TERM_DROP; break; }
+    if (digit == kDigitDropped) {
+      tl = level - 1;
+      tk = TERM_DROP;
+      if (tl == 0) atomicAdd(&counters[3], 1);   // outside the root box
+      break;
+    }
   }
   khi[k] = h;
   klo[k] = l;
@@ -851,7 +856,7 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
     OV_LAUNCHED();
     OV_TRY_CUDA(cudaGetLastError());
   }
-  int hc[3] = {0, 0, 0};
+  int hc[4] = {0, 0, 0, 0};
   OV_TRY_CUDA(cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, st));
   OV_TRY_CUDA(cudaStreamSynchronize(st));
   if (hc[1]) {
@@ -861,6 +866,9 @@ bool ov_tree_build(ov_state_impl* s, const double* pos, OvTree* T) {
   }
   const int na = hc[0];
   T->n_nodes = na;
+  // a node outside the root box takes digit 8 at level 1, so these nodes
+  // sort after every node inside it: the last n_drop_root of the order
+  T->n_drop_root = hc[3];
   // radix sort over the high word (8 passes of 8 bits), stable; vals_alt's
   // second half holds the sorted term codes, so the values alternate with a
   // separate scratch.  The sorted data ends back in khi / vals.
