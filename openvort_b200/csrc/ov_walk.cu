@@ -955,8 +955,10 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
   }
   // one rank's share: a contiguous range of the key order (each target's
   // walk depends only on its own position, so the range changes no result)
+  int key_lo = 0;   // key position of order[0]
   if (own_tree && k_count >= 0) {
     const int lo = std::min(std::max(k0, 0), n_t);
+    key_lo = lo;
     n_t = std::min(k_count, n_t - lo);
     order += lo;
     if (n_t <= 0) {
@@ -971,9 +973,11 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
   // union of their trees, and as the last block it ran almost alone at the
   // end of the launch: 20 such nodes made a 1M-point walk 28% longer.  Each
   // gets a warp of its own at the front of the list instead (the other lanes
-  // empty); the sums do not depend on the order.
-  if (own_tree && k_count < 0 && t->n_drop_root > 0 && t->n_drop_root <= kMaxDropWarps) {
-    const int nd = t->n_drop_root, nin = n_t - nd;
+  // empty); the sums do not depend on the order.  In a rank's share of the
+  // key order these nodes are the share's last ones.
+  const int nd = own_tree ? std::max(0, std::min(n_t, key_lo + n_t - (t->n_nodes - t->n_drop_root))) : 0;
+  if (nd > 0 && t->n_drop_root <= kMaxDropWarps) {
+    const int nin = n_t - nd;
     const int m = 32 * nd + nin;
     if (!t->walk_order.reserve(sizeof(int) * (size_t)m)) return false;
     k_drop_first<<<(m + 255) / 256, 256, 0, s->stream>>>(order, nin, nd, t->walk_order.as<int>());

@@ -68,6 +68,27 @@ def run_ranks(ov, t, world, steps, own_buffer=False):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
+def test_sharded_steps_with_nodes_outside_the_box(ov, precision):
+    """Nodes just outside the root box sort last in the key order, so the
+    last rank's share holds them, and its walk gives each a warp of its own:
+    3 ranks still equal one run bit for bit."""
+    t, p = tangle_and_params()
+    a = np.nonzero(t.active)[0]
+    for ax in range(3):
+        k = a[np.argmin(t.pos[a, ax])]
+        t.pos[k, ax] = -1e-6
+        k = a[np.argmax(t.pos[a, ax])]
+        t.pos[k, ax] = 0.1 + 1e-6
+    ov.configure(p, precision)
+    ref = ov.DeviceState(t.copy())
+    ref.run(0.0, DT, 2)
+    ref.download()
+    act = t.active
+    for st in run_ranks(ov, t, 3, 2):
+        assert np.array_equal(st.t.pos[act], ref.t.pos[act])
+
+
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("world", [1, 3])
 def test_sharded_steps_equal_one_run(ov, precision, world):
     t, p = tangle_and_params()
