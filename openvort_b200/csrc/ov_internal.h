@@ -97,6 +97,10 @@ struct OvTree {
   DevBuf scan_part;     // block sums of the exclusive scans
   DevBuf mom_part;      // per-chunk partial moments of the largest cells
   DevBuf walk_order;    // the walk's target list when nodes lie outside the root box
+  // the multi-image walk's groups of 32 targets by decreasing time in the
+  // last walk (wvals after the sort), their times, and the sort's buffers
+  DevBuf warp_cost, wkeys, wkeys2, wvals, wvals2, whist, wscan;
+  int n_perm_warps = 0;   // groups the order in wvals covers (0: none yet)
 };
 
 // ---------------------------------------------------------------- state

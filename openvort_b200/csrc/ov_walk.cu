@@ -684,12 +684,18 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
     k_walk_multi(
     OvParams P, TreeView T, const int* __restrict__ order, const int2* __restrict__ status,
     const double* __restrict__ pos, int n_t, unsigned combos, ImageShortcut S, double near2,
-    double* v_nl, double* v_img, unsigned long long* counters) {
+    double* v_nl, double* v_img, unsigned long long* counters, const int* __restrict__ warp_perm,
+    unsigned* __restrict__ warp_cost) {
   __shared__ unsigned sh_mask[kMultiWarps][kLevelSlots][32];
   const unsigned FULL = 0xffffffffu;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int gw = blockIdx.x * kMultiWarps + warp;
-  if (gw * 32 >= n_t) return;   // whole warp out of range
+  const long long t_start = clock64();
+  const int slot = blockIdx.x * kMultiWarps + warp;
+  if (slot * 32 >= n_t) return;   // whole warp out of range
+  // the group of 32 consecutive targets this warp takes: launch slot
+  // `slot` runs group warp_perm[slot] (the groups by decreasing time in the
+  // previous evaluation), or group `slot`
+  const int gw = warp_perm ? warp_perm[slot] : slot;
   const int i = gw * 32 + lane;
   const int k = i < n_t ? (order ? order[i] : i) : -1;
   const bool live = k >= 0 && status[k].x != OV_PINNED && status[k].x != OV_EMPTY;
@@ -830,6 +836,8 @@ __global__ void __launch_bounds__(kMultiWarps * 32, kMixed ? OV_WALK_MULTI_MIN_B
     atomicAdd(&counters[0], a);
     atomicAdd(&counters[1], b);
     atomicAdd(&counters[2], (unsigned long long)n_iter);
+    // this group's time in SM cycles / 64, for the next evaluation's order
+    if (warp_cost) warp_cost[gw] = (unsigned)min((clock64() - t_start) >> 6, 0xffffffffll);
   }
 }
 
@@ -927,6 +935,14 @@ static __global__ void k_drop_first(const int* __restrict__ perm, int nin, int n
   const int pad = 32 * nd;
   if (i >= pad + nin) return;
   out[i] = i < pad ? ((i & 31) == 0 ? perm[nin + (i >> 5)] : -1) : perm[i - pad];
+}
+
+// sort keys for the groups' order: decreasing time first
+static __global__ void k_cost_keys(const unsigned* __restrict__ cost, int n, uint64_t* keys, int* vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  keys[i] = (uint64_t)(0xffffffffu - cost[i]);
+  vals[i] = i;
 }
 
 static bool read_counters(ov_state_impl* s, OvTree* t) {
@@ -1033,15 +1049,44 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
   if (multi) {
     int warps = (n_t + 31) / 32;
     int blocks = (warps + kMultiWarps - 1) / kMultiWarps;
+    // Longest groups first: the launch runs the groups of 32 targets in the
+    // order of their times in the previous walk of this tree (the same
+    // regions of the key order, a few node moves apart), so the slow ones
+    // do not start in the last wave.  The sums do not depend on the order.
+    // A full evaluation only (a rank's share keeps the key order).
+    const bool timed = own_tree && k_count < 0;
+    const int* wperm = timed && t->n_perm_warps == warps ? t->wvals.as<int>() : nullptr;
+    unsigned* wcost = nullptr;
+    if (timed) {
+      if (!t->warp_cost.reserve(sizeof(unsigned) * (size_t)warps)) return false;
+      wcost = t->warp_cost.as<unsigned>();
+    }
     if (mixed) {
       k_walk_multi<true><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
-          P, tv, order, s->status.as<int2>(), pos, n_t, combos, sc, near2, v_nl, v_img, ctr);
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, sc, near2, v_nl, v_img, ctr, wperm, wcost);
       OV_LAUNCHED();
     } else {
       k_walk_multi<false><<<blocks, kMultiWarps * 32, 0, s->stream>>>(
-          P, tv, order, s->status.as<int2>(), pos, n_t, combos, sc, near2, v_nl, v_img, ctr);
+          P, tv, order, s->status.as<int2>(), pos, n_t, combos, sc, near2, v_nl, v_img, ctr, wperm, wcost);
       OV_LAUNCHED();
     }
+    OV_TRY_CUDA(cudaGetLastError());
+    cudaEventRecord(s->ev2, s->stream);
+    if (timed) {
+      // the order for the next walk (after the timed kernel)
+      const size_t nw = (size_t)warps;
+      if (!t->wkeys.reserve(sizeof(uint64_t) * nw) || !t->wkeys2.reserve(sizeof(uint64_t) * nw) ||
+          !t->wvals.reserve(sizeof(int) * nw) || !t->wvals2.reserve(sizeof(int) * nw))
+        return false;
+      k_cost_keys<<<(warps + 255) / 256, 256, 0, s->stream>>>(wcost, warps, t->wkeys.as<uint64_t>(),
+                                                                t->wvals.as<int>());
+      OV_LAUNCHED();
+      if (!ov_radix_sort_u64(t->wkeys.as<uint64_t>(), t->wvals.as<int>(), t->wkeys2.as<uint64_t>(),
+                             t->wvals2.as<int>(), warps, t->whist, t->wscan, s->stream))
+        return false;
+      t->n_perm_warps = warps;
+    }
+    return read_counters(s, t);
   } else {
     int warps = (n_t + 31) / 32;
     int blocks = (warps * 32 + 127) / 128;
