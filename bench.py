@@ -57,11 +57,11 @@ def _hbm_peak():
 HBM_PEAK, HBM_PEAK_SOURCE = _hbm_peak()
 FLOPS_CELL = 60.0  # per multipole evaluation (monopole + second-order terms + opening test)
 # dram__bytes_read.sum + dram__bytes_write.sum of one mixed walk launch per
-# point: 52.3 MB over 198,002 points in the ncu capture of this kernel on
+# point: 52.8 MB over 198,002 points in the ncu capture of this kernel on
 # this generator (profiles/bh_walk_multi_mixed_200k.md), scaled by the points
-WALK_DRAM_BYTES_PER_POINT = 264.0
+WALK_DRAM_BYTES_PER_POINT = 267.0
 WALK_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_walk_multi<mixed> at "
-                       "198,002 points (profiles/bh_walk_multi_mixed_200k.md), 264 B per point x points")
+                       "198,002 points (profiles/bh_walk_multi_mixed_200k.md), 267 B per point x points")
 
 
 def parse():
