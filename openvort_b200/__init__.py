@@ -13,7 +13,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import OV_FIELD_ALL, OV_PREC_FP64, OV_PREC_MIXED, OVError, check, load, stats
+from ._lib import (OV_FIELD_ALL, OV_FIELD_DXI, OV_FIELD_NORMALS, OV_FIELD_POS, OV_FIELD_TANGENTS, OV_FIELD_VELS,
+                   OV_FIELD_VS, OV_PREC_FP64, OV_PREC_MIXED, OVError, check, load, stats)
 from .tangle import EMPTY, FREE, PINNED, PINNED_SLIP, Flow, HostTangle, Params
 
 __all__ = [

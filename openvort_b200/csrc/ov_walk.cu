@@ -1053,8 +1053,9 @@ bool ov_tree_walk_nodes(ov_state_impl* s, OvTree* t, const double* pos, bool own
     // order of their times in the previous walk of this tree (the same
     // regions of the key order, a few node moves apart), so the slow ones
     // do not start in the last wave.  The sums do not depend on the order.
-    // A full evaluation only (a rank's share keeps the key order).
-    const bool timed = own_tree && k_count < 0;
+    // A rank's share of a sharded evaluation is the same key range at every
+    // evaluation, so its groups are ordered the same way.
+    const bool timed = own_tree;
     const int* wperm = timed && t->n_perm_warps == warps ? t->wvals.as<int>() : nullptr;
     unsigned* wcost = nullptr;
     if (timed) {
