@@ -674,6 +674,17 @@ __global__ void k_add3(const double* a, const double* b, double* o, int n) {
 static bool ensure_segtab(ov_state_impl* s, const double* pos);
 bool ov_segment_table(ov_state_impl* s, const double* pos) { return ensure_segtab(s, pos); }
 
+// resident blocks per SM of a kernel at a block size (0 when unknown)
+template <class K>
+static int resident_blocks(K kernel, int threads) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+
 static bool ensure_segtab(ov_state_impl* s, const double* pos) {
   if (!s->seg64.reserve(sizeof(double) * 6 * (size_t)s->n)) return false;
   if (!s->segid.reserve(sizeof(int) * (size_t)s->n)) return false;
@@ -689,8 +700,15 @@ static bool ensure_segtab(ov_state_impl* s, const double* pos) {
 // tangle still fills the GPU (about `per_sm` blocks per SM, at most
 // `max_splits` splits), each split a whole number of tiles of `tile`
 // sources; returns the sources per split.
+//
+// With `resident` (the kernel's resident blocks per SM) the split count is
+// then raised, by at most 4x, to the one whose last wave of blocks is
+// fullest: the blocks of one launch all take the same time, so a grid of
+// 3.2 waves runs as long as 4.  (On the 22.4k-point tangle the two-source
+// form had 2376 blocks against 740 resident, 20% of its time in the last,
+// partly empty wave.)
 static int source_chunk(int n_src, long long blocks, int tile, int* splits, int per_sm = 4,
-                        int max_splits = 16) {
+                        int max_splits = 16, int resident = 0) {
   static int sms = 0;
   if (!sms) {
     int dev = 0;
@@ -699,6 +717,22 @@ static int source_chunk(int n_src, long long blocks, int tile, int* splits, int 
   }
   long long want = ((long long)per_sm * sms + blocks - 1) / std::max(1LL, blocks);
   int sp = (int)std::min<long long>(max_splits, std::max<long long>(1, want));
+  if (resident > 0) {
+    const int tiles = std::max(1, (n_src + tile - 1) / tile);   // at least a tile per split
+    const int top = std::min(std::min(max_splits, 4 * sp), std::max(sp, tiles));
+    const double slots = (double)resident * sms;
+    double best = -1;
+    int best_sp = sp;
+    for (int c = sp; c <= top; ++c) {
+      const double waves = (double)blocks * c / slots;
+      const double fill = waves / std::ceil(waves);
+      if (fill > best + 1e-3) {
+        best = fill;
+        best_sp = c;
+      }
+    }
+    sp = best_sp;
+  }
   int chunk = (n_src + sp - 1) / sp;
   chunk = std::max(tile, (chunk + tile - 1) / tile * tile);
   *splits = std::max(1, (n_src + chunk - 1) / chunk);
@@ -733,7 +767,10 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
     const int bx = (n_t + kPTgt - 1) / kPTgt;
     // sources: every slot in slot order, or the sorted active nodes
     const int n_src = slot_order ? s->n : s->tree.n_nodes;
-    const int chunk = source_chunk(n_src, (long long)bx * (nimg + 1), kPSrc, &splits);
+    static const int res_chain = resident_blocks(k_direct_mixed_chain, kPB);
+    static const int res_pairs = resident_blocks(k_direct_mixed_pairs, kPB);
+    const int chunk = source_chunk(n_src, (long long)bx * (nimg + 1), kPSrc, &splits, 4, 16,
+                                   slot_order ? res_chain : res_pairs);
     if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;
     cudaEventRecord(s->ev1, s->stream);
     if (slot_order) {
@@ -750,7 +787,8 @@ bool ov_direct_nodes(ov_state_impl* s, const double* pos, double* v_nl, double* 
     // EMPTY slots are never read by the epilogue, but zero them for hygiene
   } else {
     const int bx = (s->n + kTB - 1) / kTB;
-    const int chunk = source_chunk(s->n, (long long)bx * (nimg + 1), kCS, &splits);
+    static const int res64 = resident_blocks(k_direct64_chain<false>, kTB);
+    const int chunk = source_chunk(s->n, (long long)bx * (nimg + 1), kCS, &splits, 4, 16, res64);
     if (!s->img_part.reserve(sizeof(double) * 3 * (size_t)s->n * (nimg + 1) * splits)) return false;
     cudaEventRecord(s->ev1, s->stream);
     k_direct64_chain<false><<<dim3(bx, nimg + 1, splits), kTB, 0, s->stream>>>(
@@ -779,7 +817,8 @@ bool ov_direct_points(ov_state_impl* s, const double* pos, int npts, const doubl
   // four waves of the kernel's 7 resident blocks per SM
   const int bx = (npts + kTB - 1) / kTB;
   int splits = 1;
-  const int chunk = source_chunk(std::max(1, n_src), (long long)bx * (nimg + 1), kTS, &splits, 32, 64);
+  static const int res64 = resident_blocks(k_direct64_chain<true>, kTB);
+  const int chunk = source_chunk(std::max(1, n_src), (long long)bx * (nimg + 1), kTS, &splits, 32, 64, res64);
   size_t bytes = sizeof(double) * 3 * (size_t)npts * (nimg + 1) * splits;
   if (!s->img_part.reserve(bytes)) return false;
   dim3 grid(bx, nimg + 1, splits);
@@ -814,7 +853,8 @@ bool ov_direct_points_bounded(ov_state_impl* s, const double* pos, int npts, con
   int splits = 1;
   // a few thousand points: about eight waves of the kernel's 4 resident
   // blocks per SM, so the last wave's tail is a small share
-  const int chunk = source_chunk(std::max(1, s->n), (long long)bx * (nimg + 1), kPSrc, &splits, 32, 64);
+  static const int res_pts = resident_blocks(k_direct_mixed_points, kPB);
+  const int chunk = source_chunk(std::max(1, s->n), (long long)bx * (nimg + 1), kPSrc, &splits, 32, 64, res_pts);
   const size_t slabs = (size_t)(nimg + 1) * splits;
   // per-image partial sums (3 per point) followed by the bound partials
   if (!s->img_part.reserve(sizeof(double) * 4 * (size_t)npts * slabs)) return false;
