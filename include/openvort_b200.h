@@ -489,7 +489,9 @@ int ov_reconnect_vortices(struct tangle_state *tangle, double t, double rec_dist
  * takes the approach test's Biot-Savart sums with the FP32 far field and a
  * bound on their error per node; a test whose sign that bound leaves open
  * is taken again with FP64 sums, so links, flags and count are the FP64
- * form's, and the velocities it writes carry the mixed form's error.
+ * form's, and the velocities it writes carry the mixed form's error.  The
+ * environment variable OV_RECONNECT_MARGIN_SCALE multiplies that margin (a
+ * huge value sends every test to the FP64 re-check; for tests).
  * Counters of the last ov_reconnect_vortices call on this thread: */
 typedef struct {
   int candidates;     /* pairs that passed the static tests */
