@@ -74,7 +74,7 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.5)
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--dt", type=float, default=1e-6)
-    ap.add_argument("--fp64-steps", type=int, default=1)
+    ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip the direct-sum and batch lines")
